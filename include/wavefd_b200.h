@@ -1,0 +1,294 @@
+/*
+ * WaveFD-B200: the C ABI of the B200 (sm_100a) propagator library.
+ *
+ * Part 1 declares the drop-in surface: the same extern "C" names, argument lists and meaning as
+ * the reference's shared libraries, so that WaveFD's Julia ccall layer (or any other binding)
+ * can load this library in their place. Each block cites the reference file it replaces.
+ * Contract kept from the reference: calls are synchronous and return nothing; the object owns
+ * every array; getters return pointers the caller reads and writes between calls (here CUDA
+ * managed memory, so host code may dereference them); objects are not re-entrant.
+ *
+ * Part 2 declares add-on entry points that the reference does not have (status reporting,
+ * asynchronous stepping, device-resident source/receiver tables).
+ *
+ * Memory layout everywhere: k = (kx*ny + ky)*nz + kz, i.e. a column-major (nz,ny,nx) Julia array.
+ */
+#ifndef WAVEFD_B200_H
+#define WAVEFD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================================== */
+/* Part 1: drop-in surface                                                                  */
+/* ======================================================================================== */
+
+/* ---- src/prop3DAcoIsoDenQ_DEO2_FDTD.cc:6-140 ---- */
+void *Prop3DAcoIsoDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long ny, long nz, long nsponge, float dx,
+                                       float dy, float dz, float dt, long nbx, long nby, long nbz);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_free(void *p);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_VB(void *p, float *dVel, float *dBuoy, float *wavefieldP,
+                                                        float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_B(void *p, float *dBuoy, float *wavefieldP, float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_VB(void *p, float *dVel, float *dBuoy, float *wavefieldP,
+                                                           float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_B(void *p, float *dBuoy, float *wavefieldP,
+                                                          float *wavefieldDP);
+void Prop3DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep(void *p, float *dVel, float *wavefieldDP,
+                                                                     const long isFWI);
+long Prop3DAcoIsoDenQ_DEO2_FDTD_getNx(void *p);
+long Prop3DAcoIsoDenQ_DEO2_FDTD_getNy(void *p);
+long Prop3DAcoIsoDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getV(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getB(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop3DAcoIsoDenQ_DEO2_FDTD_getPOld(void *p);
+
+/* ---- src/prop3DAcoVTIDenQ_DEO2_FDTD.cc:6-157 (getDtOmegaInvQ is an addition) ---- */
+void *Prop3DAcoVTIDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long ny, long nz, long nsponge, float dx,
+                                       float dy, float dz, float dt, long nbx, long nby, long nbz);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_free(void *p);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_TimeStepLinear(void *p);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP, float *wavefieldDM);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_ForwardBornInjection_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                         float *wavefieldP, float *wavefieldM, float *wavefieldDP,
+                                                         float *wavefieldDM);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP,
+                                                          float *wavefieldDM);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep_V(void *p, float *dVel, float *wavefieldDP,
+                                                                       float *wavefieldDM, const long isFWI);
+void Prop3DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                            float *wavefieldP, float *wavefieldM,
+                                                            float *wavefieldDP, float *wavefieldDM);
+long Prop3DAcoVTIDenQ_DEO2_FDTD_getNx(void *p);
+long Prop3DAcoVTIDenQ_DEO2_FDTD_getNy(void *p);
+long Prop3DAcoVTIDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getV(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getEps(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getEta(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getB(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getF(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getMSpace(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getPOld(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getMCur(void *p);
+float *Prop3DAcoVTIDenQ_DEO2_FDTD_getMOld(void *p);
+
+/* ---- src/prop3DAcoTTIDenQ_DEO2_FDTD.cc:6-180 ---- */
+void *Prop3DAcoTTIDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long ny, long nz, long nsponge, float dx,
+                                       float dy, float dz, float dt, long nbx, long nby, long nbz);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_free(void *p);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP, float *wavefieldDM);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_ForwardBornInjection_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                         float *wavefieldP, float *wavefieldM, float *wavefieldDP,
+                                                         float *wavefieldDM);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP,
+                                                          float *wavefieldDM);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep_V(void *p, float *dVel, float *wavefieldDP,
+                                                                       float *wavefieldDM, const long isFWI);
+void Prop3DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                            float *wavefieldP, float *wavefieldM,
+                                                            float *wavefieldDP, float *wavefieldDM);
+long Prop3DAcoTTIDenQ_DEO2_FDTD_getNx(void *p);
+long Prop3DAcoTTIDenQ_DEO2_FDTD_getNy(void *p);
+long Prop3DAcoTTIDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getV(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getEps(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getEta(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getSinTheta(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getCosTheta(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getSinPhi(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getCosPhi(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getB(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getF(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getMSpace(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getPOld(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getMCur(void *p);
+float *Prop3DAcoTTIDenQ_DEO2_FDTD_getMOld(void *p);
+
+/* ---- src/prop2DAcoIsoDenQ_DEO2_FDTD.cc:6-131 ---- */
+void *Prop2DAcoIsoDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long nz, long nsponge, float dx, float dz,
+                                       float dt, long nbx, long nbz);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_free(void *p);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_VB(void *p, float *dVel, float *dBuoy, float *wavefieldP,
+                                                        float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_ForwardBornInjection_B(void *p, float *dBuoy, float *wavefieldP, float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_VB(void *p, float *dVel, float *dBuoy, float *wavefieldP,
+                                                           float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_B(void *p, float *dBuoy, float *wavefieldP,
+                                                          float *wavefieldDP);
+void Prop2DAcoIsoDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep(void *p, float *dVel, float *wavefieldDP,
+                                                                     const long isFWI);
+long Prop2DAcoIsoDenQ_DEO2_FDTD_getNx(void *p);
+long Prop2DAcoIsoDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getV(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getB(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop2DAcoIsoDenQ_DEO2_FDTD_getPOld(void *p);
+
+/* ---- src/prop2DAcoVTIDenQ_DEO2_FDTD.cc:6-176 ---- */
+void *Prop2DAcoVTIDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long nz, long nsponge, float dx, float dz,
+                                       float dt, long nbx, long nbz);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_free(void *p);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_TimeStepLinear(void *p);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP, float *wavefieldDM);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_ForwardBornInjection_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                         float *wavefieldP, float *wavefieldM, float *wavefieldDP,
+                                                         float *wavefieldDM);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP,
+                                                          float *wavefieldDM);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep_V(void *p, float *dVel, float *wavefieldDP,
+                                                                       float *wavefieldDM, const long isFWI);
+void Prop2DAcoVTIDenQ_DEO2_FDTD_AdjointBornAccumulation_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                            float *wavefieldP, float *wavefieldM,
+                                                            float *wavefieldDP, float *wavefieldDM);
+long Prop2DAcoVTIDenQ_DEO2_FDTD_getNx(void *p);
+long Prop2DAcoVTIDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getV(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getEps(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getEta(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getB(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getF(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getMSpace(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getPOld(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getMCur(void *p);
+float *Prop2DAcoVTIDenQ_DEO2_FDTD_getMOld(void *p);
+/* src/prop2DAcoVTIDenQ_DEO2_FDTD.cc:158-176 */
+void Prop2DAcoVTIDenQ_DEO2_FDTD_applyFirstDerivatives2D_PlusHalf(
+    const long freeSurface, const long nx, const long nz, const long nthread, const float c8_1, const float c8_2,
+    const float c8_3, const float c8_4, const float invDx, const float invDz, const float *inX, const float *inZ,
+    float *outX, float *outZ, const long BX_2D, const long BZ_2D);
+
+/* ---- src/prop2DAcoTTIDenQ_DEO2_FDTD.cc:6-161 ---- */
+void *Prop2DAcoTTIDenQ_DEO2_FDTD_alloc(long fs, long nthread, long nx, long nz, long nsponge, float dx, float dz,
+                                       float dt, long nbx, long nbz);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_free(void *p);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_SetupDtOmegaInvQ(void *p, float freqQ, float qMin, float qInterior);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_TimeStep(void *p);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_ScaleSpatialDerivatives(void *p);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_ForwardBornInjection_V(void *p, float *dVel, float *wavefieldDP, float *wavefieldDM);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_ForwardBornInjection_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                         float *wavefieldP, float *wavefieldM, float *wavefieldDP,
+                                                         float *wavefieldDM);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_V(void *p, float *dVel, float *wavefieldDP,
+                                                          float *wavefieldDM);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_wavefieldsep_V(void *p, float *dVel, float *wavefieldDP,
+                                                                       float *wavefieldDM, const long isFWI);
+void Prop2DAcoTTIDenQ_DEO2_FDTD_AdjointBornAccumulation_VEA(void *p, float *dVel, float *dEps, float *dEta,
+                                                            float *wavefieldP, float *wavefieldM,
+                                                            float *wavefieldDP, float *wavefieldDM);
+long Prop2DAcoTTIDenQ_DEO2_FDTD_getNx(void *p);
+long Prop2DAcoTTIDenQ_DEO2_FDTD_getNz(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getV(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getEps(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getEta(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getSinTheta(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getCosTheta(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getB(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getF(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getDtOmegaInvQ(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getPSpace(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getMSpace(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getPCur(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getPOld(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getMCur(void *p);
+float *Prop2DAcoTTIDenQ_DEO2_FDTD_getMOld(void *p);
+
+/* ---- src/spacetime.cc:132-204 (and src/spacetime.jl:793-808 for the point types) ---- */
+typedef struct SourcePoint32 {
+    long iu;  /* 1-based linear grid index */
+    long ir;  /* 1-based trace index */
+    float c;  /* weight */
+} SourcePoint32;
+typedef struct SourcePoint64 {
+    long iu;
+    long ir;
+    double c;
+} SourcePoint64;
+void injectdata_float(float *field, float *data, size_t it, size_t nt, SourcePoint32 **partitions,
+                      size_t npartitions, long *npoints_per_partition, size_t nthreads);
+void injectdata_double(double *field, double *data, size_t it, size_t nt, SourcePoint64 **partitions,
+                       size_t npartitions, long *npoints_per_partition, size_t nthreads);
+void extractdata_float(float *data, float *field, SourcePoint32 **partitions, size_t npartitions,
+                       long *npoints_per_partition, size_t it, size_t nt, size_t nthreads);
+void extractdata_double(double *data, double *field, SourcePoint64 **partitions, size_t npartitions,
+                        long *npoints_per_partition, size_t it, size_t nt, size_t nthreads);
+
+/* ======================================================================================== */
+/* Part 2: add-on entry points (no counterpart in the reference)                            */
+/* ======================================================================================== */
+
+/* status codes */
+#define WFD_OK 0
+#define WFD_ERR_CUDA 1
+#define WFD_ERR_ALLOC 2
+#define WFD_ERR_ARG 3
+#define WFD_ERR_UNSUPPORTED 4
+#define WFD_ERR_TIMEOUT 5
+
+/* last error of calls that have no object (alloc, spacetime), and of a given object */
+int WFD_LastError(void);
+const char *WFD_LastErrorMessage(void);
+int WFD_Prop_Status(void *p);
+const char *WFD_Prop_Message(void *p);
+
+/* 1 = bitwise-parity kernels (IEEE order, no FMA), 0 = fast kernels (default) */
+int WFD_Prop_SetStrict(void *p, int strict);
+/* 1 = fused single-sweep step kernels where available (default), 0 = the two-pass kernels */
+int WFD_Prop_SetFused(void *p, int fused);
+/* enqueue nsteps time steps (linear != 0: TimeStepLinear) without host synchronisation */
+int WFD_Prop_TimeStepAsync(void *p, long nsteps, int linear);
+int WFD_Prop_Synchronize(void *p);
+/* move every array of the object to device memory (after host writes through the getters) */
+int WFD_Prop_Prefetch(void *p);
+/* the object's CUDA stream (a cudaStream_t) */
+void *WFD_Prop_Stream(void *p);
+/* device-resident source/receiver tables built from a flat point list (grouped by written
+ * location, contributions accumulated in list order, as the reference does partition-wise) */
+void *WFD_Points_Create(const SourcePoint32 *points, long npoints, int by_receiver);
+void WFD_Points_Free(void *table);
+long WFD_Points_Groups(void *table);
+/* field[iu-1] += c * data[(ir-1)*nt + it-1] on the device; data column-major (nt, ntraces) */
+int WFD_Inject(void *table, float *field, const float *data, long it, long nt, void *stream);
+/* data[(ir-1)*nt + it-1] += c * field[iu-1] on the device */
+int WFD_Extract(void *table, float *data, const float *field, long it, long nt, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVEFD_B200_H */

@@ -1,0 +1,114 @@
+"""Injection/extraction on the GPU against the oracle (bitwise): the drop-in libspacetime
+entry points with host and managed arrays, and the device-resident point tables."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests.harness import fptr, mismatch_report, same
+from wavefd_b200.abi import SourcePoint32, SpacetimeABI
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from wavefd_b200 import _lib
+    return _lib.library()
+
+
+def _points(n, ngrid, nr, seed, sort_by="iu"):
+    rng = np.random.default_rng(seed)
+    iu = rng.integers(1, ngrid + 1, n)
+    ir = rng.integers(1, nr + 1, n)
+    c = rng.standard_normal(n).astype(np.float32)
+    order = np.argsort(iu if sort_by == "iu" else ir, kind="stable")
+    return iu[order], ir[order], c[order]
+
+
+def _partitions(key, iu, ir, c, nparts):
+    """Split into contiguous partitions the way source_blocking does (equal keys kept together)."""
+    n = len(c)
+    bounds = [0]
+    step = max(1, n // nparts)
+    while bounds[-1] < n:
+        b = min(n, bounds[-1] + step)
+        while b < n and key[b] == key[b - 1]:
+            b += 1
+        bounds.append(b)
+    parts = []
+    keep = []
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        arr = (SourcePoint32 * (b - a))(*[SourcePoint32(int(iu[i]), int(ir[i]), float(c[i])) for i in range(a, b)])
+        keep.append(arr)
+        parts.append(ctypes.cast(arr, ctypes.POINTER(SourcePoint32)))
+    pp = (ctypes.POINTER(SourcePoint32) * len(parts))(*parts)
+    npp = (ctypes.c_long * len(parts))(*[b - a for a, b in zip(bounds[:-1], bounds[1:])])
+    return pp, npp, len(parts), keep
+
+
+@pytest.mark.parametrize("nparts", [1, 4])
+def test_dropin_inject_extract_host_arrays(lib, oracle, nparts):
+    st = SpacetimeABI(lib)
+    ngrid, nr, nt = 4000, 9, 17
+    iu, ir, c = _points(3000, ngrid, nr, 7)
+    pp, npp, npart, keep = _partitions(iu, iu, ir, c, nparts)
+    rng = np.random.default_rng(8)
+    data = rng.standard_normal(nr * nt).astype(np.float32)
+    field = rng.standard_normal(ngrid).astype(np.float32)
+    f_gpu, f_or = field.copy(), field.copy()
+    st.injectdata_float(fptr(f_gpu), fptr(data), 4, nt, pp, npart, npp, 4)
+    oracle.inject(f_or, data, 4, nt, iu, ir, c)
+    assert same(f_gpu, f_or), mismatch_report(f_gpu, f_or)
+    iu2, ir2, c2 = _points(3000, ngrid, nr, 9, sort_by="ir")
+    pp2, npp2, npart2, keep2 = _partitions(ir2, iu2, ir2, c2, nparts)
+    d_gpu, d_or = data.copy(), data.copy()
+    st.extractdata_float(fptr(d_gpu), fptr(field), pp2, npart2, npp2, 11, nt, 4)
+    oracle.extract(d_or, field, 11, nt, iu2, ir2, c2)
+    assert same(d_gpu, d_or), mismatch_report(d_gpu, d_or)
+
+
+def test_dropin_inject_into_managed_field(lib, oracle):
+    from wavefd_b200.props import PCur, Prop3DAcoIsoDenQ_DEO2_FDTD, free
+    prop = Prop3DAcoIsoDenQ_DEO2_FDTD(nz=24, ny=20, nx=22, dz=10, dy=10, dx=10, dt=0.001)
+    pcur = PCur(prop)
+    rng = np.random.default_rng(3)
+    pcur[...] = rng.standard_normal(pcur.shape).astype(np.float32)
+    flat = pcur.reshape(-1)
+    ref = flat.copy()
+    st = SpacetimeABI(lib)
+    iu, ir, c = _points(500, flat.size, 3, 4)
+    pp, npp, npart, keep = _partitions(iu, iu, ir, c, 2)
+    nt = 6
+    data = rng.standard_normal(3 * nt).astype(np.float32)
+    st.injectdata_float(flat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), fptr(data), 2, nt, pp, npart, npp, 2)
+    oracle.inject(ref, data, 2, nt, iu, ir, c)
+    assert same(flat, ref), mismatch_report(flat, ref)
+    free(prop)
+
+
+def test_device_tables_inject_extract(lib, oracle):
+    import torch
+    ngrid, nr, nt = 5000, 11, 13
+    iu, ir, c = _points(4000, ngrid, nr, 21)
+    pts = (SourcePoint32 * len(c))(*[SourcePoint32(int(a), int(b), float(x)) for a, b, x in zip(iu, ir, c)])
+    tin = lib.WFD_Points_Create(pts, len(c), 0)
+    tout = lib.WFD_Points_Create(pts, len(c), 1)
+    assert tin and tout
+    rng = np.random.default_rng(22)
+    data = rng.standard_normal(nr * nt).astype(np.float32)
+    field = rng.standard_normal(ngrid).astype(np.float32)
+    fd = torch.from_numpy(field).cuda()
+    dd = torch.from_numpy(data).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.WFD_Inject(tin, ctypes.c_void_p(fd.data_ptr()), ctypes.c_void_p(dd.data_ptr()), 5, nt, ctypes.c_void_p(s)) == 0
+    assert lib.WFD_Extract(tout, ctypes.c_void_p(dd.data_ptr()), ctypes.c_void_p(fd.data_ptr()), 6, nt, ctypes.c_void_p(s)) == 0
+    torch.cuda.synchronize()
+    f_or, d_or = field.copy(), data.copy()
+    oracle.inject(f_or, data, 5, nt, iu, ir, c)
+    o2 = np.argsort(ir, kind="stable")
+    oracle.extract(d_or, f_or, 6, nt, iu[o2], ir[o2], c[o2])
+    assert same(fd.cpu().numpy(), f_or)
+    assert same(dd.cpu().numpy(), d_or)
+    lib.WFD_Points_Free(tin)
+    lib.WFD_Points_Free(tout)

@@ -74,6 +74,9 @@ class PropagatorABI:
         fn("getNz", c_long, [c_void_p])
         for g in self.getters:
             fn("get" + g, _f32p, [c_void_p])
+        if "DtOmegaInvQ" not in self.getters and self.has("getDtOmegaInvQ"):
+            # exported by the CUDA build for every propagator, absent from the reference's 3D VTI library
+            fn("getDtOmegaInvQ", _f32p, [c_void_p])
         for v in self.born:
             fn("ForwardBornInjection_" + v, None, [c_void_p] + [_f32p] * _born_args(self.physics, v))
         for v in self.images:

@@ -1,0 +1,65 @@
+// Add-on entry points of the C ABI (status, modes, asynchronous stepping, prefetch).
+#include <string>
+
+#include "../../include/wavefd_b200.h"
+#include "wfd_prop.h"
+
+using wfd::Prop;
+
+namespace {
+Prop *P(void *p) { return reinterpret_cast<Prop *>(p); }
+thread_local std::string t_msg;
+}  // namespace
+
+extern "C" int WFD_LastError(void) { return wfd::global_error(nullptr); }
+
+extern "C" const char *WFD_LastErrorMessage(void) {
+    wfd::global_error(&t_msg);
+    return t_msg.c_str();
+}
+
+extern "C" int WFD_Prop_Status(void *p) { return p ? P(p)->status : WFD_ERR_ARG; }
+
+extern "C" const char *WFD_Prop_Message(void *p) { return p ? P(p)->message.c_str() : "null object"; }
+
+extern "C" int WFD_Prop_SetStrict(void *p, int strict) {
+    if (!p) return WFD_ERR_ARG;
+    P(p)->strict = strict != 0;
+    return WFD_OK;
+}
+
+extern "C" int WFD_Prop_SetFused(void *p, int fused) {
+    if (!p) return WFD_ERR_ARG;
+    P(p)->fused = fused != 0;
+    return WFD_OK;
+}
+
+extern "C" int WFD_Prop_TimeStepAsync(void *p, long nsteps, int linear) {
+    if (!p || nsteps < 0) return WFD_ERR_ARG;
+    if (linear && P(p)->phys != wfd::VTI) return wfd::prop_fail(P(p), WFD_ERR_UNSUPPORTED, "linear step is VTI only");
+    for (long i = 0; i < nsteps; i++) {
+        int rc = wfd::prop_step(P(p), linear != 0, false);
+        if (rc) return rc;
+    }
+    return WFD_OK;
+}
+
+extern "C" int WFD_Prop_Synchronize(void *p) { return p ? wfd::prop_sync(P(p)) : WFD_ERR_ARG; }
+
+extern "C" int WFD_Prop_Prefetch(void *p) {
+    if (!p) return WFD_ERR_ARG;
+    Prop *q = P(p);
+    const size_t bytes = sizeof(float) * (size_t)q->ncells();
+    for (int f = 0; f < wfd::F_COUNT; f++) {
+        if (!q->field[f]) continue;
+#if CUDART_VERSION >= 13000
+        cudaMemLocation loc{cudaMemLocationTypeDevice, q->device};
+        cudaMemPrefetchAsync(q->field[f], bytes, loc, 0, q->stream);
+#else
+        cudaMemPrefetchAsync(q->field[f], bytes, q->device, q->stream);
+#endif
+    }
+    return wfd::prop_sync(q);
+}
+
+extern "C" void *WFD_Prop_Stream(void *p) { return p ? (void *)P(p)->stream : nullptr; }

@@ -1,0 +1,13 @@
+// Selection of the fused single-sweep step kernels by physics and dimension.
+#include "wfd_kernels.h"
+
+namespace WFD_NS {
+using namespace wfd;
+
+bool fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
+    (void)linear;
+    if (g.ndim == 3 && phys == ISO) return fused_iso3d(g, F, s);
+    return false;
+}
+
+}  // namespace WFD_NS

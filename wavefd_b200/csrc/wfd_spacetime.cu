@@ -1,0 +1,299 @@
+// Source injection and receiver extraction (spacetime.cc:144-204), on the GPU.
+//
+// The reference runs its partitions in parallel (no grid point, resp. trace, is shared between
+// two partitions: src/spacetime.jl:1087-1129) and each partition sequentially, so every grid
+// cell (resp. trace sample) receives its contributions in partition order. Here the points are
+// grouped by the cell they write (stable sort, which keeps that order) and one thread owns each
+// group and accumulates it in order with separate IEEE multiply and add: the result is the
+// reference's, bit for bit, whatever the grouping into partitions was.
+//
+// Drop-in entry points take host partition tables, as the reference does, and work for device,
+// managed or host field/data arrays. The WFD_Points_* add-ons keep the grouped table resident
+// on the device for the time loop.
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "../../include/wavefd_b200.h"
+#include "wfd_prop.h"
+
+namespace wfd {
+
+namespace {
+
+template <class T>
+struct PointsT {
+    long iu, ir;
+    T c;
+};
+
+// one group per written location: key = 0-based index written, other = 0-based index read
+template <class T>
+struct Table {
+    long npoints = 0, ngroups = 0;
+    int by_receiver = 0;
+    std::vector<long> key, start, other;
+    std::vector<T> c;
+    // device copies
+    long *d_key = nullptr, *d_start = nullptr, *d_other = nullptr;
+    T *d_c = nullptr;
+};
+
+template <class T>
+void build(Table<T> &t, const std::vector<PointsT<T>> &pts, int by_receiver) {
+    t.npoints = (long)pts.size();
+    t.by_receiver = by_receiver;
+    std::vector<long> order(pts.size());
+    std::iota(order.begin(), order.end(), 0L);
+    auto keyof = [&](long i) { return by_receiver ? pts[i].ir : pts[i].iu; };
+    std::stable_sort(order.begin(), order.end(), [&](long a, long b) { return keyof(a) < keyof(b); });
+    t.key.clear();
+    t.start.clear();
+    t.other.resize(pts.size());
+    t.c.resize(pts.size());
+    for (size_t j = 0; j < order.size(); j++) {
+        const auto &p = pts[order[j]];
+        const long k = by_receiver ? p.ir : p.iu;
+        if (j == 0 || k != keyof(order[j - 1])) {
+            t.key.push_back(k - 1);
+            t.start.push_back((long)j);
+        }
+        t.other[j] = (by_receiver ? p.iu : p.ir) - 1;
+        t.c[j] = p.c;
+    }
+    t.start.push_back((long)order.size());
+    t.ngroups = (long)t.key.size();
+}
+
+template <class T>
+bool upload(Table<T> &t, cudaStream_t s) {
+    const size_t ng = (size_t)t.ngroups, np = (size_t)t.npoints;
+    if (cudaMallocAsync(&t.d_key, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
+    if (cudaMallocAsync(&t.d_start, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
+    if (cudaMallocAsync(&t.d_other, sizeof(long) * (np + 1), s) != cudaSuccess) return false;
+    if (cudaMallocAsync(&t.d_c, sizeof(T) * (np + 1), s) != cudaSuccess) return false;
+    if (ng) cudaMemcpyAsync(t.d_key, t.key.data(), sizeof(long) * ng, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(t.d_start, t.start.data(), sizeof(long) * (ng + 1), cudaMemcpyHostToDevice, s);
+    if (np) cudaMemcpyAsync(t.d_other, t.other.data(), sizeof(long) * np, cudaMemcpyHostToDevice, s);
+    if (np) cudaMemcpyAsync(t.d_c, t.c.data(), sizeof(T) * np, cudaMemcpyHostToDevice, s);
+    return true;
+}
+
+template <class T>
+void release(Table<T> &t, cudaStream_t s) {
+    if (t.d_key) cudaFreeAsync(t.d_key, s);
+    if (t.d_start) cudaFreeAsync(t.d_start, s);
+    if (t.d_other) cudaFreeAsync(t.d_other, s);
+    if (t.d_c) cudaFreeAsync(t.d_c, s);
+    t.d_key = t.d_start = t.d_other = nullptr;
+    t.d_c = nullptr;
+}
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// dst[key[g]] (+)= sum over the group of c * src[other * stride + off], in group order.
+// With dst/src given as compact arrays (stride 0 / per-point values) the same kernel serves the
+// staged drop-in path.
+template <class T>
+__global__ void k_scatter_groups(long ngroups, const long *__restrict__ key, const long *__restrict__ start,
+                                 const long *__restrict__ other, const T *__restrict__ c, T *dst, long dst_stride,
+                                 long dst_off, int dst_compact, const T *__restrict__ src, long src_stride,
+                                 long src_off, int src_compact) {
+    const long gi = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= ngroups) return;
+    const long d = dst_compact ? gi : key[gi] * dst_stride + dst_off;
+    T acc = dst[d];
+    for (long j = start[gi]; j < start[gi + 1]; j++) {
+        const T v = src_compact ? src[j] : src[other[j] * src_stride + src_off];
+        acc = add_rn(acc, mul_rn(c[j], v));
+    }
+    dst[d] = acc;
+}
+
+template <class T>
+__global__ void k_gather(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
+                         T *dst) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i] * stride + off];
+}
+
+template <class T>
+__global__ void k_scatter(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
+                          T *dst) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[idx[i] * stride + off] = src[i];
+}
+
+inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
+
+template <class T>
+std::vector<PointsT<T>> flatten(void **partitions, size_t npartitions, const long *npoints) {
+    std::vector<PointsT<T>> pts;
+    size_t total = 0;
+    for (size_t i = 0; i < npartitions; i++) total += (size_t)npoints[i];
+    pts.reserve(total);
+    for (size_t i = 0; i < npartitions; i++) {
+        const PointsT<T> *p = reinterpret_cast<const PointsT<T> *>(partitions[i]);
+        for (long j = 0; j < npoints[i]; j++) pts.push_back(p[j]);
+    }
+    return pts;
+}
+
+cudaStream_t st_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    return s;
+}
+
+// Drop-in inject (by_receiver = 0) / extract (1). dst is written at key*dst_stride + dst_off,
+// src is read at other*src_stride + src_off.
+template <class T>
+void dropin(int by_receiver, T *dst, long dst_stride, long dst_off, const T *src, long src_stride, long src_off,
+            void **partitions, size_t npartitions, const long *npoints) {
+    std::vector<PointsT<T>> pts = flatten<T>(partitions, npartitions, npoints);
+    if (pts.empty()) return;
+    cudaStream_t s = st_stream();
+    Table<T> t;
+    build(t, pts, by_receiver);
+    if (!upload(t, s)) {
+        set_global_error(WFD_ERR_ALLOC, "point table allocation failed");
+        release(t, s);
+        return;
+    }
+    const bool dst_dev = device_accessible(dst);
+    const bool src_dev = device_accessible(src);
+    const long ng = t.ngroups, np = t.npoints;
+    T *d_dst = nullptr, *d_src = nullptr;
+    cudaMallocAsync(&d_dst, sizeof(T) * (size_t)ng, s);
+    // current values of the written locations
+    if (dst_dev) {
+        k_gather<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, dst_stride, dst_off, dst, d_dst);
+    } else {
+        std::vector<T> h((size_t)ng);
+        for (long g = 0; g < ng; g++) h[g] = dst[t.key[g] * dst_stride + dst_off];
+        cudaMemcpyAsync(d_dst, h.data(), sizeof(T) * (size_t)ng, cudaMemcpyHostToDevice, s);
+        cudaStreamSynchronize(s);
+    }
+    // values read by every point
+    cudaMallocAsync(&d_src, sizeof(T) * (size_t)np, s);
+    std::vector<T> hs;
+    if (src_dev) {
+        k_gather<T><<<nb(np), 256, 0, s>>>(np, t.d_other, src_stride, src_off, src, d_src);
+    } else {
+        hs.resize((size_t)np);
+        for (long j = 0; j < np; j++) hs[j] = src[t.other[j] * src_stride + src_off];
+        cudaMemcpyAsync(d_src, hs.data(), sizeof(T) * (size_t)np, cudaMemcpyHostToDevice, s);
+    }
+    k_scatter_groups<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, t.d_start, t.d_other, t.d_c, d_dst, 0, 0, 1, d_src, 0,
+                                               0, 1);
+    if (dst_dev) {
+        k_scatter<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, dst_stride, dst_off, d_dst, dst);
+        cudaStreamSynchronize(s);
+    } else {
+        std::vector<T> h((size_t)ng);
+        cudaMemcpyAsync(h.data(), d_dst, sizeof(T) * (size_t)ng, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        for (long g = 0; g < ng; g++) dst[t.key[g] * dst_stride + dst_off] = h[g];
+    }
+    cudaFreeAsync(d_dst, s);
+    cudaFreeAsync(d_src, s);
+    release(t, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) set_global_error(WFD_ERR_CUDA, cudaGetErrorString(e));
+}
+
+struct DeviceTable {
+    Table<float> t;
+};
+
+}  // namespace
+}  // namespace wfd
+
+using wfd::DeviceTable;
+
+// ---- drop-in libspacetime exports (spacetime.cc:144-204) ---------------------------------------------
+extern "C" void injectdata_float(float *field, float *data, size_t it, size_t nt, SourcePoint32 **partitions,
+                                 size_t npartitions, long *npoints_per_partition, size_t nthreads) {
+    (void)nthreads;
+    wfd::dropin<float>(0, field, 1, 0, data, (long)nt, (long)it - 1, (void **)partitions, npartitions,
+                       npoints_per_partition);
+}
+
+extern "C" void injectdata_double(double *field, double *data, size_t it, size_t nt, SourcePoint64 **partitions,
+                                  size_t npartitions, long *npoints_per_partition, size_t nthreads) {
+    (void)nthreads;
+    wfd::dropin<double>(0, field, 1, 0, data, (long)nt, (long)it - 1, (void **)partitions, npartitions,
+                        npoints_per_partition);
+}
+
+extern "C" void extractdata_float(float *data, float *field, SourcePoint32 **partitions, size_t npartitions,
+                                  long *npoints_per_partition, size_t it, size_t nt, size_t nthreads) {
+    (void)nthreads;
+    wfd::dropin<float>(1, data, (long)nt, (long)it - 1, field, 1, 0, (void **)partitions, npartitions,
+                       npoints_per_partition);
+}
+
+extern "C" void extractdata_double(double *data, double *field, SourcePoint64 **partitions, size_t npartitions,
+                                   long *npoints_per_partition, size_t it, size_t nt, size_t nthreads) {
+    (void)nthreads;
+    wfd::dropin<double>(1, data, (long)nt, (long)it - 1, field, 1, 0, (void **)partitions, npartitions,
+                        npoints_per_partition);
+}
+
+// ---- add-on: device-resident point tables ------------------------------------------------------------
+extern "C" void *WFD_Points_Create(const SourcePoint32 *points, long npoints, int by_receiver) {
+    if (npoints < 0 || (npoints > 0 && !points)) {
+        wfd::set_global_error(WFD_ERR_ARG, "WFD_Points_Create: bad point list");
+        return nullptr;
+    }
+    std::vector<wfd::PointsT<float>> pts((size_t)npoints);
+    for (long i = 0; i < npoints; i++) pts[i] = {points[i].iu, points[i].ir, points[i].c};
+    DeviceTable *d = new DeviceTable();
+    wfd::build(d->t, pts, by_receiver);
+    cudaStream_t s = wfd::st_stream();
+    if (!wfd::upload(d->t, s) || cudaStreamSynchronize(s) != cudaSuccess) {
+        wfd::release(d->t, s);
+        delete d;
+        wfd::set_global_error(WFD_ERR_ALLOC, "WFD_Points_Create: device allocation failed");
+        return nullptr;
+    }
+    return d;
+}
+
+extern "C" void WFD_Points_Free(void *table) {
+    DeviceTable *d = reinterpret_cast<DeviceTable *>(table);
+    if (!d) return;
+    cudaStream_t s = wfd::st_stream();
+    wfd::release(d->t, s);
+    cudaStreamSynchronize(s);
+    delete d;
+}
+
+extern "C" long WFD_Points_Groups(void *table) {
+    DeviceTable *d = reinterpret_cast<DeviceTable *>(table);
+    return d ? d->t.ngroups : -1;
+}
+
+extern "C" int WFD_Inject(void *table, float *field, const float *data, long it, long nt, void *stream) {
+    DeviceTable *d = reinterpret_cast<DeviceTable *>(table);
+    if (!d || d->t.by_receiver || it < 1 || it > nt) return WFD_ERR_ARG;
+    if (!d->t.ngroups) return WFD_OK;
+    wfd::k_scatter_groups<float><<<wfd::nb(d->t.ngroups), 256, 0, (cudaStream_t)stream>>>(
+        d->t.ngroups, d->t.d_key, d->t.d_start, d->t.d_other, d->t.d_c, field, 1, 0, 0, data, nt, it - 1, 0);
+    return cudaGetLastError() == cudaSuccess ? WFD_OK : WFD_ERR_CUDA;
+}
+
+extern "C" int WFD_Extract(void *table, float *data, const float *field, long it, long nt, void *stream) {
+    DeviceTable *d = reinterpret_cast<DeviceTable *>(table);
+    if (!d || !d->t.by_receiver || it < 1 || it > nt) return WFD_ERR_ARG;
+    if (!d->t.ngroups) return WFD_OK;
+    wfd::k_scatter_groups<float><<<wfd::nb(d->t.ngroups), 256, 0, (cudaStream_t)stream>>>(
+        d->t.ngroups, d->t.d_key, d->t.d_start, d->t.d_other, d->t.d_c, data, nt, it - 1, 0, field, 1, 0, 0);
+    return cudaGetLastError() == cudaSuccess ? WFD_OK : WFD_ERR_CUDA;
+}
