@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Headline benchmark: Mcells/s and % of the HBM roofline of the 3D visco-acoustic time step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload iso512|tti400]
+
+A "step" is one time step of the single-shot forward workload: the propagator step, the injection
+of the source sample and the extraction of the receiver samples of that time index. Default
+workload: 3D AcoIsoDenQ forward, 512^3 cells, 10 m, dt 0.5 ms, 40-cell sponge, 12 Hz Ricker source
+at the centre, 256 x 256 surface receivers (synthetic, seeded). Inputs are resident in HBM and far
+larger than L2 (537 MB per field). Under torchrun each rank runs its own shot (weak scaling, no
+collective on the data path); value = all ranks' cells x steps / the slowest rank's time.
+
+--impl reference times the reference's own C++/OpenMP implementation (compiled from its sources into
+oracle/_ref) on the host cores for the same workload and prints the same JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "iso512": dict(physics="iso", name="Prop3DAcoIsoDenQ_DEO2_FDTD", shape=(512, 512, 512), d=10.0, dt=0.0005,
+                   nt=1000, nsponge=40, fpeak=12.0, nrec=(256, 256), bytes_per_cell=28,
+                   label="3D AcoIsoDenQ single-shot forward, 512^3 (134M cells), 10 m, dt 0.5 ms, nt 1000, "
+                         "40-cell sponge, 12 Hz Ricker, 256x256 surface receivers"),
+    # profiling-size case of the same kernel (fields still larger than L2: 67 MB each)
+    "iso256": dict(physics="iso", name="Prop3DAcoIsoDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
+                   nt=1000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=28,
+                   label="3D AcoIsoDenQ forward, 256^3 (16.8M cells), profiling size"),
+    "tti400": dict(physics="tti", name="Prop3DAcoTTIDenQ_DEO2_FDTD", shape=(400, 400, 400), d=10.0, dt=0.0005,
+                   nt=2000, nsponge=40, fpeak=12.0, nrec=(256, 256), bytes_per_cell=72,
+                   label="3D AcoTTIDenQ forward, 400^3 (64M cells), 10 m, dt 0.5 ms, nt 2000, 40-cell sponge, "
+                         "12 Hz Ricker, 256x256 surface receivers"),
+}
+METRIC = "Mcells/s & %HBM roofline, 3D Iso/TTI step; Born image s/shot learned vs plain"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def profiled_traffic(kernel_key):
+    """Per-launch DRAM bytes from the committed ncu summary, if one exists for this kernel."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        j = json.load(f)
+    return j.get(kernel_key)
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = f"/tmp/wfd_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------------------------
+def run_ours(args, W):
+    import torch
+
+    from wavefd_b200 import _lib, props, synthetic
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = _lib.library()
+    nx, ny, nz = W["shape"]
+    ncells = nx * ny * nz
+    cls = getattr(props, W["name"])
+    prop = cls(nz=nz, ny=ny, nx=nx, nsponge=W["nsponge"], dz=W["d"], dy=W["d"], dx=W["d"], dt=W["dt"],
+               freesurface=True, freqQ=5.0, qMin=0.1, qInterior=100.0)
+    model = synthetic.earth_model((nx, ny, nz), W["physics"], seed=1 + rank, d=W["d"], dt=W["dt"],
+                                  nsponge=W["nsponge"], device="cuda")
+    # write the model into the object's managed arrays on the device (no host round trip)
+    for k, t in model.items():
+        dst = _managed_tensor(prop, k, (nx, ny, nz))
+        dst.copy_(t)
+    del model
+    torch.cuda.synchronize()
+    prop.prefetch()
+    stream = torch.cuda.ExternalStream(prop.stream())
+    sptr = ctypes.c_void_p(prop.stream())
+    # acquisition
+    src = synthetic.center_source((nx, ny, nz), W["d"])
+    rec = synthetic.surface_receivers((nx, ny, nz), W["nrec"][0], W["nrec"][1], W["nsponge"])
+    from wavefd_b200.abi import SourcePoint32
+    tsrc = lib.WFD_Points_Create(src.ctypes.data_as(ctypes.POINTER(SourcePoint32)), len(src), 0)
+    trec = lib.WFD_Points_Create(rec.ctypes.data_as(ctypes.POINTER(SourcePoint32)), len(rec), 1)
+    nt = W["nt"]
+    from wavefd_b200.spacetime import causal_ricker
+    wav = torch.from_numpy(causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"])).cuda()
+    nrec = len(rec)
+    traces = torch.zeros(nrec * nt, device="cuda")
+    pcur_name = "PCur"
+
+    def step(it):
+        _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
+        pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+        _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, sptr), "inject")
+        _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(traces.data_ptr()), pc, it, nt, sptr), "extract")
+
+    K, Wu = args.steps, args.warmup
+    it = 0
+    for _ in range(Wu):
+        it = it % nt + 1
+        step(it)
+    prop.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    # -- device-timed region: K full steps, plus per-step events around the step kernel(s) -------------
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for i in range(K):
+            it = it % nt + 1
+            kev[i][0].record(stream)
+            _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
+            kev[i][1].record(stream)
+            pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+            _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, sptr), "inject")
+            _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(traces.data_ptr()), pc, it, nt, sptr), "extract")
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    kms = [a.elapsed_time(b) for a, b in kev]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_per_step = ms / K
+    value = world * ncells * K / (ms / 1e3) / 1e6
+    # -- end-to-end through the public API with host buffers: per step the source sample goes up
+    #    from pinned memory and the receiver samples of that step come back to pinned memory -------
+    h_wav = torch.from_numpy(causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"])).pin_memory()
+    h_rec = torch.empty(nrec, pin_memory=True)
+    d_sample = torch.zeros(1, device="cuda")
+    d_rec = torch.zeros(nrec, device="cuda")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for i in range(K):
+            it = it % nt + 1
+            d_sample.copy_(h_wav[it - 1:it], non_blocking=True)
+            _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
+            pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+            _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(d_sample.data_ptr()), 1, 1, sptr), "inject")
+            d_rec.zero_()
+            _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(d_rec.data_ptr()), pc, 1, 1, sptr), "extract")
+            h_rec.copy_(d_rec, non_blocking=True)
+            stream.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * ncells * K / t_e2e / 1e6
+    # -- roofline of the step kernel(s) --------------------------------------------------------------
+    kern_ms = statistics.mean(kms)
+    alg_bytes = W["bytes_per_cell"] * ncells
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    peak, peak_src = peaks()
+    traffic = profiled_traffic(W["name"])
+    launches_per_step = 1 if prop.physics == "iso" else 2
+    clocks = clk.summary()
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "Mcells/s", "n_gpus": world, "steps": K, "warmup": Wu,
+        "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded layered+random earth model, Gardner density, block Q)",
+        "config": {"workload": W["label"], "grid": list(W["shape"]), "time_steps_per_shot": nt,
+                   "l2": "inputs larger than L2 (537 MB per field at 512^3)", "parallelism": f"shots x{world}"},
+        "e2e": {"value": round(e2e, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * nrec},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "step kernel(s) of " + W["name"], "algorithmic_bytes_per_cell": W["bytes_per_cell"],
+                     "kernel_ms": round(kern_ms, 4), "peak_source": peak_src},
+        "gpu_launches": K * (launches_per_step + 2),
+        "clocks": clocks,
+    }
+    # tensors used on the object's stream go before the stream does
+    del traces, wav, d_sample, d_rec, h_rec, h_wav
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    lib.WFD_Points_Free(tsrc)
+    lib.WFD_Points_Free(trec)
+    props.free(prop)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(W)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def _managed_tensor(prop, getter, shape):
+    import torch
+    ptr = ctypes.cast(getattr(prop.abi, "get" + getter)(prop.p), ctypes.c_void_p).value
+
+    class _CAI:
+        __cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4", "data": (ptr, False), "version": 3,
+                                    "strides": None}
+    return torch.as_tensor(_CAI(), device="cuda")
+
+
+# ---------------------------------------------------------------------------------------------------
+def _ref_flavour():
+    from oracle.oracle import reference_lib_path
+    for fl in ("avx2", "fast"):
+        if os.path.exists(reference_lib_path("prop3DAcoIsoDenQ_DEO2_FDTD", fl)):
+            if fl == "avx2":
+                flags = open("/proc/cpuinfo").read()
+                if " avx2" not in flags or " fma" not in flags:
+                    continue
+            return fl
+    return None
+
+
+def _cpu_run(W, nsteps_max, seconds, warmup=1, with_acq=True):
+    """Reference propagator on the host cores (oracle/_ref): returns (Mcells/s, steps, threads, flavour)."""
+    from oracle.oracle import reference_lib
+    from wavefd_b200.abi import PropagatorABI, SpacetimeABI
+    fl = _ref_flavour()
+    if fl is None:
+        return None
+    name = W["name"]
+    lib = reference_lib(name.replace("Prop", "prop"), fl)
+    abi = PropagatorABI(lib, name)
+    nx, ny, nz = W["shape"]
+    th = os.cpu_count() or 1
+    p = abi.alloc(1, th, nx, ny, nz, W["nsponge"], W["d"], W["d"], W["d"], W["dt"], 8, 8, nz)
+    abi.SetupDtOmegaInvQ(p, 5.0, 0.1, 100.0)
+    shp = (nx, ny, nz)
+    arr = lambda g: np.ctypeslib.as_array(getattr(abi, "get" + g)(p), shape=shp)
+    arr("V")[...] = np.linspace(1500, 4500, nz, dtype=np.float32)[None, None, :]
+    arr("B")[...] = 0.5
+    if W["physics"] != "iso":
+        arr("Eps")[...] = 0.1
+        arr("Eta")[...] = 0.05
+        arr("F")[...] = 0.85
+    if W["physics"] == "tti":
+        for g, v in (("SinTheta", 0.3), ("CosTheta", 0.954), ("SinPhi", 0.5), ("CosPhi", 0.866)):
+            arr(g)[...] = v
+    rng = np.random.default_rng(0)
+    arr("PCur")[:, :, :64] = rng.standard_normal((nx, ny, 64)).astype(np.float32) * 1e-3
+    st = None
+    if with_acq:
+        from wavefd_b200 import synthetic
+        from wavefd_b200.abi import SourcePoint32
+        st = SpacetimeABI(reference_lib("spacetime", fl))
+        src = synthetic.center_source(shp, W["d"])
+        rec = synthetic.surface_receivers(shp, W["nrec"][0], W["nrec"][1], W["nsponge"])
+        from wavefd_b200.spacetime import receiver_blocking, source_blocking, _partition_args
+        sb, rb = source_blocking(src, th), receiver_blocking(rec, th)
+        sp, sc = _partition_args(sb)
+        rp, rc = _partition_args(rb)
+        nt = W["nt"]
+        from wavefd_b200.spacetime import causal_ricker
+        wav = causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"])
+        traces = np.zeros(len(rec) * nt, np.float32)
+        fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    it = 0
+
+    def one():
+        nonlocal it
+        it = it % W["nt"] + 1
+        abi.TimeStep(p)
+        if st is not None:
+            pc = abi.getPCur(p)
+            st.injectdata_float(pc, fp(wav), it, nt, sp, len(sb), sc, th)
+            st.extractdata_float(fp(traces), pc, rp, len(rb), rc, it, nt, th)
+
+    for _ in range(warmup):
+        one()
+    n, t0 = 0, time.perf_counter()
+    times = []
+    while n < nsteps_max and (time.perf_counter() - t0) < seconds:
+        t1 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t1)
+        n += 1
+    abi.free(p)
+    return nx * ny * nz / statistics.median(times) / 1e6, n, th, fl, times
+
+
+def cpu_baseline(W):
+    r = _cpu_run(W, nsteps_max=50, seconds=15.0)
+    if r is None:
+        return {"value": None, "unit": "Mcells/s", "cores": None, "kind": "reference",
+                "sample": "reference library not built"}
+    v, n, th, fl, _ = r
+    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+            "sample": f"{W['name']} TimeStep + injectdata_float + extractdata_float on the full "
+                      f"{'x'.join(map(str, W['shape']))} grid, median of {n} steps after 1 warm-up, "
+                      f"{th} OpenMP threads, reference built with -O3 -ffast-math ({fl})"}
+
+
+def run_reference(args, W):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if _ref_flavour() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
+        return
+    r = _cpu_run(W, nsteps_max=args.steps, seconds=1e9, warmup=args.warmup)
+    v, n, th, fl, times = r
+    ms = statistics.mean(times) * 1e3
+    out = {
+        "metric": METRIC, "value": round(v, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": n, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": W["label"], "grid": list(W["shape"]), "parallelism": f"OpenMP x{th}"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+                         "sample": f"{n} full-grid steps (TimeStep + inject + extract), median"},
+        "e2e": {"value": round(v, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="iso512", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    W = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, W)
+    else:
+        run_ours(args, W)
+    # leave without running interpreter-teardown destructors (CUDA objects owned by two runtimes)
+    sys.stdout.flush()
+    sys.stderr.flush()
+    os._exit(0)
+
+
+if __name__ == "__main__":
+    main()

@@ -9,7 +9,7 @@ import numpy as np
 
 from wavefd_b200.abi import PROPAGATORS, PropagatorABI
 
-SMALL_SHAPES = {2: (44, 1, 38), 3: (26, 22, 24)}  # (nz, ny, nx)
+SMALL_SHAPES = {2: (44, 1, 38), 3: (28, 22, 24)}  # (nz, ny, nx); nz*4 a multiple of 16 (TMA rows)
 
 
 def geometry(name):

@@ -26,7 +26,7 @@ def library() -> ctypes.CDLL:
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             raise WaveFDError(f"CUDA library not built: {LIB_PATH} (run python -m wavefd_b200.build)")
-        lib = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+        lib = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_LOCAL)
         _declare(lib)
         _lib = lib
     return _lib

@@ -30,8 +30,10 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 STRICT = ["-DWFD_STRICT=1", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 FAST = ["-DWFD_STRICT=0", "-fmad=true", "-prec-div=false", "-prec-sqrt=true", "-ftz=true"]
 
-KERNEL_SOURCES = ["wfd_generic.cu", "wfd_fused.cu", "wfd_fused_iso3d.cu", "wfd_wavefieldsep.cu"]
-HOST_SOURCES = ["wfd_prop.cu", "wfd_bornimage.cu", "wfd_capi.cu", "wfd_addon.cu", "wfd_spacetime.cu"]
+KERNEL_SOURCES = ["wfd_generic.cu", "wfd_fused.cu", "wfd_fused_iso3d.cu", "wfd_fused_iso3d_tma.cu",
+                  "wfd_wavefieldsep.cu"]
+HOST_SOURCES = ["wfd_prop.cu", "wfd_bornimage.cu", "wfd_capi.cu", "wfd_addon.cu", "wfd_spacetime.cu",
+                "wfd_tma_host.cu"]
 
 REFERENCE_NAMES = ["prop2DAcoIsoDenQ_DEO2_FDTD", "prop2DAcoVTIDenQ_DEO2_FDTD", "prop2DAcoTTIDenQ_DEO2_FDTD",
                    "prop3DAcoIsoDenQ_DEO2_FDTD", "prop3DAcoVTIDenQ_DEO2_FDTD", "prop3DAcoTTIDenQ_DEO2_FDTD",
@@ -77,7 +79,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         objs = list(ex.map(_compile, jobs))
     tmp = out + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcuda"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "shared", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -35,6 +35,8 @@ struct Scratch {
     void dplus3(const wfd::Grid &g, const float *inx, const float *iny, const float *inz, float *ox,     \
                 float *oy, float *oz, cudaStream_t s);                                                   \
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
+    bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
+    unsigned fused_status_and_clear();                                                                   \
     void dminus3(const wfd::Grid &g, const float *fx, const float *fy, const float *fz, float *ox,       \
                  float *oy, float *oz, cudaStream_t s);                                                  \
     void tti_dplus(const wfd::Grid &g, const wfd::Fields &F, const float *in, float *o1, float *o2,      \

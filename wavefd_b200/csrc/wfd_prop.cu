@@ -267,7 +267,13 @@ void prop_setup_q(Prop *p, float freqQ, float qMin, float qInterior) {
 }
 
 // ---------------------------------------------------------------------------------------------
-int prop_sync(Prop *p) { return check_cuda(p, cudaStreamSynchronize(p->stream), "synchronize"); }
+int prop_sync(Prop *p) {
+    if (int rc = check_cuda(p, cudaStreamSynchronize(p->stream), "synchronize")) return rc;
+    // device status words of the TMA kernels: a bounded wait that ran out
+    if (wfd_fast::fused_status_and_clear() | wfd_strict::fused_status_and_clear())
+        return prop_fail(p, WFD_ERR_TIMEOUT, "a fused step kernel timed out waiting for its tile loads");
+    return WFD_OK;
+}
 
 int prop_step(Prop *p, bool linear, bool sync) {
     Grid g = p->grid();
