@@ -11,7 +11,8 @@ from ctypes import POINTER, c_int, c_long, c_void_p
 from .abi import SourcePoint32
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libwavefd_b200.so")
+# WAVEFD_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("WAVEFD_B200_LIB") or os.path.join(HERE, "lib", "libwavefd_b200.so")
 
 _lib = None
 

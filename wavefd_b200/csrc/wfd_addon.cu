@@ -1,7 +1,7 @@
 // Add-on entry points of the C ABI (status, modes, asynchronous stepping, prefetch).
 #include <string>
 
-#include "../../include/wavefd_b200.h"
+#include "wavefd_b200.h"
 #include "wfd_prop.h"
 
 using wfd::Prop;

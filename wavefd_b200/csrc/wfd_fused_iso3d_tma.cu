@@ -7,11 +7,16 @@
 //   B(j) with its halo (40 x 24 at z0-4, y0-4), B(j+3) (32 x 16), pOld(j), V(j), Q(j) (32 x 16).
 // pCur and B are read twice (the second time from L2), which keeps the stage small enough for
 // three CTAs per SM. A thread owns 4 consecutive z cells of one row (float4 shared-memory
-// accesses) and keeps along x register queues of pCur and of the pass-1 x output, 8 planes each.
+// accesses) and keeps along x register queues of pCur and of the pass-1 x output, 8 planes each;
+// the queue slot of plane j+i is (q+i)&7, so the queues never move (one small case per phase).
 // At plane j, warps 0-1 form the pass-1 y output on the 24 halo-extended rows (3 rows per thread,
-// sliding along y) and warps 2-3 the pass-1 z output on the 40 halo-extended columns; then every
-// thread applies D- and the time update to its 4 cells and stores pOld and pSpace as float4.
-// Tiles whose halo lies wholly inside the interior take a branch-free path.
+// sliding along y) and warps 2-3 the pass-1 z output on the 40 halo-extended columns (a run of
+// 2-3 quads per thread, sliding along z); then every thread applies D- and the time update to its
+// 4 cells and stores pOld and pSpace as float4.
+// The reference's region rules (interior [4,n-4), free-surface rows, untouched annulus) are
+// applied as selects on values computed everywhere; three code variants: interior tiles (no
+// selects), edge tiles (selects), and the top tile with a free surface (selects plus the image
+// stencils above kz = 0, which only the first z quad needs).
 // Persistent CTAs loop over (tile, x-chunk) items; a chunk starts with 14 warm-up planes that only
 // fill the queues. Waits are bounded; on timeout the kernel records an error in a device status
 // word and leaves. Requires nz % 4 == 0 (TMA row pitch); the caller falls back otherwise.
@@ -46,6 +51,8 @@ constexpr size_t SMEM_BYTES = (size_t)OFF_BAR * 4 + NS * 8 + 16;
 static_assert(OFF_BAR % 2 == 0, "mbarrier alignment");
 static_assert((STAGE * 4) % 128 == 0 && (S_BH * 4) % 128 == 0 && (S_PN * 4) % 128 == 0, "TMA destination alignment");
 
+enum Mode { INNER = 0, EDGE = 1, TOP = 2 };
+
 __device__ unsigned int d_status;
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -60,14 +67,22 @@ __device__ __forceinline__ float st8(const Grid &g, float w0, float w1, float w2
     return g.c1 * (-w3 + w4) + g.c2 * (-w2 + w5) + g.c3 * (-w1 + w6) + g.c4 * (-w0 + w7);
 }
 
+// cells of the pass-1 outputs that the reference computes: interior, or free-surface rows 1..3
+// (row 0 holds B*0 = 0 for the x/y outputs)
+__device__ __forceinline__ bool xy_out_z(const Grid &g, int zz) {
+    return zz < g.nz - 4 && (zz >= 4 || (g.fs && zz > 0));
+}
+// cells of the pass-1 z output and of the update: interior, or free-surface rows 0..3
+__device__ __forceinline__ bool z_out_z(const Grid &g, int zz) { return zz >= 0 && zz < g.nz - 4 && (zz >= 4 || g.fs); }
+__device__ __forceinline__ bool y_in(const Grid &g, int y) { return y >= 4 && y < g.ny - 4; }
+
 // pass-1 y/z outputs of the centre plane j into TYs/TZs
-template <bool INTERIOR>
-__device__ __forceinline__ void ext_stage(const Grid &g, const long j, const int z0, const int y0, const float *st,
-                                          float *TYs, float *TZs) {
+template <int MODE>
+__device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const bool top, const int z0, const int y0,
+                                          const float *st, float *TYs, float *TZs) {
     const int tid = threadIdx.x;
     const float *Pc = st + S_PH;
     const float *Bc = st + S_BH;
-    const bool xin = INTERIOR || (j >= 4 && j < g.nx - 4);
     if (tid < 64) {
         const int zq = tid & 7;
         const int r0 = (tid >> 3) * 3;  // rows r0..r0+2 of the 24 extended rows
@@ -79,56 +94,56 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const long j, const int
 #pragma unroll
         for (int rr = 0; rr < 3; rr++) {
             const int r = r0 + rr;
-            const int y = y0 - 4 + r;
-            const bool ok = INTERIOR || (xin && y >= 4 && y < g.ny - 4);
+            const bool rowok = xin && y_in(g, y0 - 4 + r);
             const float4 b = ld4(Bc + r * BZW + 4 + 4 * zq);
             float out[4];
 #pragma unroll
             for (int m = 0; m < 4; m++) {
-                const int zz = zz0 + m;
-                float t = 0.0f;
-                // region 1, or free-surface rows 1..3 (row 0 holds B*0 = 0)
-                if (INTERIOR || (ok && zz < g.nz - 4 && (zz >= 4 || (g.fs && zz > 0)))) {
-                    const float s = st8(g, at(w[rr], m), at(w[rr + 1], m), at(w[rr + 2], m), at(w[rr + 3], m),
-                                        at(w[rr + 4], m), at(w[rr + 5], m), at(w[rr + 6], m), at(w[rr + 7], m));
-                    t = at(b, m) * (g.idy * s);
-                }
+                const float s = st8(g, at(w[rr], m), at(w[rr + 1], m), at(w[rr + 2], m), at(w[rr + 3], m),
+                                    at(w[rr + 4], m), at(w[rr + 5], m), at(w[rr + 6], m), at(w[rr + 7], m));
+                float t = at(b, m) * (g.idy * s);
+                if (MODE != INNER) t = (rowok && xy_out_z(g, zz0 + m)) ? t : 0.0f;
                 out[m] = t;
             }
             st4(TYs + r * TZ + 4 * zq, make_float4(out[0], out[1], out[2], out[3]));
         }
     } else {
-        // 16 rows x 10 quads = 160 items over 64 threads
+        // 16 rows x 10 quads over 64 threads: 4 threads per row, quads {0,1,2} {3,4,5} {6,7} {8,9},
+        // each thread sliding along z over its contiguous quads
+        const int tt = tid - 64;
+        const int r = tt >> 2;
+        const int g4 = tt & 3;
+        const int qa = g4 == 0 ? 0 : (g4 == 1 ? 3 : (g4 == 2 ? 6 : 8));
+        const int nq = g4 < 2 ? 3 : 2;
+        const bool rowok = xin && y_in(g, y0 + r);
+        const float *rowp = Pc + (r + 7) * PZW;
+        float v[20];
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            const float4 a = (i < nq + 2) ? ld4(rowp + 4 * (qa + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[4 * i] = a.x;
+            v[4 * i + 1] = a.y;
+            v[4 * i + 2] = a.z;
+            v[4 * i + 3] = a.w;
+        }
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const int item = tid - 64 + 64 * k;
-            if (item >= TY * (TZW / 4)) break;
-            const int r = item / (TZW / 4);
-            const int qi = item - r * (TZW / 4);
-            const int y = y0 + r;
+            if (k >= nq) break;
+            const int qi = qa + k;
             const int zb = z0 - 4 + 4 * qi;  // first z of this quad
-            const bool ok = INTERIOR || (xin && y >= 4 && y < g.ny - 4);
-            const float *rowp = Pc + (r + 7) * PZW;
-            const float4 a0 = ld4(rowp + 4 * qi), a1 = ld4(rowp + 4 * qi + 4), a2 = ld4(rowp + 4 * qi + 8);
-            const float v[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
             const float4 b = ld4(Bc + (r + 4) * BZW + 4 * qi);
             float out[4];
 #pragma unroll
             for (int m = 0; m < 4; m++) {
-                const int zz = zb + m;
-                float t = 0.0f;
-                if (INTERIOR || (ok && zz >= 0 && zz < g.nz - 4 && (zz >= 4 || g.fs))) {
-                    float s;
-                    if (INTERIOR || zz >= 3) {
-                        s = st8(g, v[m + 1], v[m + 2], v[m + 3], v[m + 4], v[m + 5], v[m + 6], v[m + 7], v[m + 8]);
-                    } else {
-                        // antisymmetric image above the free surface, p[-j] = -p[j] (z0 == 0 here)
-                        auto pm = [&](int jz) { return jz >= 0 ? rowp[jz + 8] : -rowp[-jz + 8]; };
-                        s = st8(g, pm(zz - 3), pm(zz - 2), pm(zz - 1), pm(zz), pm(zz + 1), pm(zz + 2), pm(zz + 3),
-                                pm(zz + 4));
-                    }
-                    t = at(b, m) * (g.idz * s);
+                const int o = 4 * k + m;
+                float s = st8(g, v[o + 1], v[o + 2], v[o + 3], v[o + 4], v[o + 5], v[o + 6], v[o + 7], v[o + 8]);
+                if (top && zb == 0 && m < 3) {
+                    // antisymmetric image above the free surface, p[-j] = -p[j]; column of z is z+8
+                    auto pm = [&](int jz) { return jz >= 0 ? rowp[jz + 8] : -rowp[-jz + 8]; };
+                    s = st8(g, pm(m - 3), pm(m - 2), pm(m - 1), pm(m), pm(m + 1), pm(m + 2), pm(m + 3), pm(m + 4));
                 }
+                float t = at(b, m) * (g.idz * s);
+                if (MODE != INNER) t = (rowok && z_out_z(g, zb + m)) ? t : 0.0f;
                 out[m] = t;
             }
             st4(TZs + r * TZW + 4 * qi, make_float4(out[0], out[1], out[2], out[3]));
@@ -137,12 +152,11 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const long j, const int
 }
 
 // D- in y and z, the time update and the stores of this thread's 4 cells
-template <bool INTERIOR>
-__device__ __forceinline__ void fin_stage(const Grid &g, const long j, const int z, const int y, const int zq,
-                                          const int row, const float *sx, const float *pc, const float *st,
-                                          const float *TYs, const float *TZs, float *po, float *ps) {
-    const bool xin = INTERIOR || (j >= 4 && j < g.nx - 4);
-    const bool yin = INTERIOR || (y >= 4 && y < g.ny - 4);
+template <int MODE>
+__device__ __forceinline__ void fin_stage(const Grid &g, const long j, const bool xin, const bool top, const int z,
+                                          const int y,
+                                          const int zq, const int row, const float *sx, const float *pc,
+                                          const float *st, const float *TYs, const float *TZs, float *po, float *ps) {
     const int o = row * TZ + 4 * zq;
     const float4 pold4 = ld4(st + S_PO + o), v4 = ld4(st + S_V + o), q4 = ld4(st + S_Q + o);
     const float4 b4 = ld4(st + S_BH + (4 + row) * BZW + 4 + 4 * zq);
@@ -152,34 +166,29 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const int
     const float *tzr = TZs + row * TZW;
     const float4 t0 = ld4(tzr + 4 * zq), t1 = ld4(tzr + 4 * zq + 4), t2 = ld4(tzr + 4 * zq + 8);
     const float w[12] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, t2.y, t2.z, t2.w};
+    const bool rowok = xin && y_in(g, y);
     float npo[4], nps[4];
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-        const int zz = z + m;
         const float pcv = pc[m];
         const float pov = at(pold4, m);
-        const bool r1 = INTERIOR || (xin && yin && zz >= 4 && zz < g.nz - 4);
-        const bool r2 = !INTERIOR && xin && yin && g.fs && zz < 4 && zz < g.nz - 4;
-        if (!r1 && !r2) {
-            npo[m] = pov;  // not updated
-            nps[m] = 0.0f;
-            continue;
-        }
-        float L;
-        if (!INTERIOR && r2 && zz == 0) {
-            L = 0.0f + 0.0f + 0.0f;
-        } else {
-            const float sy = st8(g, at(ty[0], m), at(ty[1], m), at(ty[2], m), at(ty[3], m), at(ty[4], m),
-                                 at(ty[5], m), at(ty[6], m), at(ty[7], m));
-            float sz;
-            if (INTERIOR || zz >= 4) {
-                sz = st8(g, w[m], w[m + 1], w[m + 2], w[m + 3], w[m + 4], w[m + 5], w[m + 6], w[m + 7]);
+        const float sy = st8(g, at(ty[0], m), at(ty[1], m), at(ty[2], m), at(ty[3], m), at(ty[4], m),
+                             at(ty[5], m), at(ty[6], m), at(ty[7], m));
+        float sz = st8(g, w[m], w[m + 1], w[m + 2], w[m + 3], w[m + 4], w[m + 5], w[m + 6], w[m + 7]);
+        float L = g.idx * sx[m] + g.idy * sy + g.idz * sz;
+        if (top && z == 0) {
+            if (m == 0) {
+                L = 0.0f + 0.0f + 0.0f;  // the free surface row: all derivatives are zero
             } else {
-                // symmetric image above the free surface, t[-j] = t[j-1] (z0 == 0: column of z is z+4)
+                // symmetric image above the free surface, t[-j] = t[j-1]; column of z is z+4
                 auto tm = [&](int jz) { return tzr[(jz >= 0 ? jz : -jz - 1) + 4]; };
-                sz = st8(g, tm(zz - 4), tm(zz - 3), tm(zz - 2), tm(zz - 1), tm(zz), tm(zz + 1), tm(zz + 2),
-                         tm(zz + 3));
+                sz = st8(g, tm(m - 4), tm(m - 3), tm(m - 2), tm(m - 1), tm(m), tm(m + 1), tm(m + 2), tm(m + 3));
+                const float dx = g.idx * sx[m];
+                const float dy = g.idy * sy;
+                const float dz = g.idz * sz;
+                L = dx + dy + dz;
             }
+        } else if (WFD_STRICT) {
             const float dx = g.idx * sx[m];
             const float dy = g.idy * sy;
             const float dz = g.idz * sz;
@@ -187,12 +196,45 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const int
         }
         const float V = at(v4, m);
         const float dt2V2_B = g.dt2 * V * V / at(b4, m);
-        npo[m] = dt2V2_B * L - at(q4, m) * (pcv - pov) - pov + 2 * pcv;
-        nps[m] = L;
+        float np = dt2V2_B * L - at(q4, m) * (pcv - pov) - pov + 2 * pcv;
+        float nl = L;
+        if (MODE != INNER) {
+            const bool ok = rowok && z_out_z(g, z + m);
+            np = ok ? np : pov;  // cells the reference leaves alone
+            nl = ok ? nl : 0.0f;
+        }
+        npo[m] = np;
+        nps[m] = nl;
     }
     const long k = j * g.sx + (long)y * g.nz + z;
     st4(po + k, make_float4(npo[0], npo[1], npo[2], npo[3]));
     st4(ps + k, make_float4(nps[0], nps[1], nps[2], nps[3]));
+}
+
+// Queue update of phase PH = q & 7: pCur(j+7) enters slot (PH+7)&7, the pass-1 x output at plane
+// j+3 enters qt slot (PH+7)&7; returns the D- x stencil at plane j and pCur(j).
+template <int PH>
+__device__ __forceinline__ void queue_phase(float (&qp)[8][4], float (&qt)[8][4], const Grid &g, const bool xin_a,
+                                            const unsigned txmask, const float4 pn, const float4 bn, float *sx,
+                                            float *pc) {
+    constexpr int N = (PH + 7) & 7;
+    qp[N][0] = pn.x;
+    qp[N][1] = pn.y;
+    qp[N][2] = pn.z;
+    qp[N][3] = pn.w;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const float s = st8(g, qp[(PH + 0) & 7][m], qp[(PH + 1) & 7][m], qp[(PH + 2) & 7][m], qp[(PH + 3) & 7][m],
+                            qp[(PH + 4) & 7][m], qp[(PH + 5) & 7][m], qp[(PH + 6) & 7][m], qp[N][m]);
+        const float t = at(bn, m) * (g.idx * s);
+        qt[N][m] = (xin_a && ((txmask >> m) & 1u)) ? t : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        sx[m] = st8(g, qt[(PH + 0) & 7][m], qt[(PH + 1) & 7][m], qt[(PH + 2) & 7][m], qt[(PH + 3) & 7][m],
+                    qt[(PH + 4) & 7][m], qt[(PH + 5) & 7][m], qt[(PH + 6) & 7][m], qt[N][m]);
+        pc[m] = qp[PH][m];
+    }
 }
 
 __global__ void __launch_bounds__(NT, 3)
@@ -238,13 +280,17 @@ __global__ void __launch_bounds__(NT, 3)
         const int z = z0 + 4 * zq;
         const int y = y0 + row;
         const bool own = z < g.nz && y < g.ny;
-        const bool yin = y >= 4 && y < g.ny - 4;
         const long xbeg = (long)chi * xchunk;
         const long xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
         const long jstart = xbeg - WARMUP;
         const int ngroups = (int)(xend - jstart);
         // the tile and its halo of extended rows/columns lie inside [4, n-4) in y and z
         const bool tile_inner = z0 - 4 >= 4 && z0 + TZ + 4 <= g.nz - 4 && y0 - 4 >= 4 && y0 + TY + 4 <= g.ny - 4;
+        const bool tile_top = z0 == 0 && g.fs;
+        unsigned txmask = 0;  // cells of this thread whose pass-1 x output is computed (given x)
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (y_in(g, y) && xy_out_z(g, z + m)) txmask |= 1u << m;
 
         auto issue = [&](long jj, unsigned gs) {
             uint64_t *bar = &bars[gs % NS];
@@ -263,7 +309,7 @@ __global__ void __launch_bounds__(NT, 3)
             out_from = gseq;
             out_to = gseq + (D < ngroups ? D : ngroups);
         }
-        // queues: qp[i] = pCur(j+i), qt[i] = pass-1 x output at plane j-4+i
+        // queues: qp[(q+i)&7] = pCur(j+i), qt[(q+i)&7] = pass-1 x output at plane j-4+i
         float qp[8][4], qt[8][4];
 #pragma unroll
         for (int i = 0; i < 8; i++)
@@ -287,52 +333,29 @@ __global__ void __launch_bounds__(NT, 3)
             }
             if (tid == 0) out_from = gs + 1;
             const float *st = sm + (gs % NS) * STAGE;
-            // ---- queues: newest pCur plane j+7, pass-1 x output at plane j+3 -----------------------
+            float sx[4], pc[4];
             {
                 const int o = row * TZ + 4 * zq;
                 const float4 pn = ld4(st + S_PN + o);
                 const float4 bn = ld4(st + S_BN + o);
-#pragma unroll
-                for (int i = 0; i < 7; i++)
-#pragma unroll
-                    for (int m = 0; m < 4; m++) qp[i][m] = qp[i + 1][m];
-                qp[7][0] = pn.x;
-                qp[7][1] = pn.y;
-                qp[7][2] = pn.z;
-                qp[7][3] = pn.w;
-                const long xa = j + 3;
-                const bool xin = xa >= 4 && xa < g.nx - 4;
-#pragma unroll
-                for (int i = 0; i < 7; i++)
-#pragma unroll
-                    for (int m = 0; m < 4; m++) qt[i][m] = qt[i + 1][m];
-#pragma unroll
-                for (int m = 0; m < 4; m++) {
-                    const int zz = z + m;
-                    float t = 0.0f;
-                    if (xin && yin && zz < g.nz - 4 && (zz >= 4 || (g.fs && zz > 0))) {
-                        const float s = st8(g, qp[0][m], qp[1][m], qp[2][m], qp[3][m], qp[4][m], qp[5][m], qp[6][m],
-                                            qp[7][m]);
-                        t = at(bn, m) * (g.idx * s);
-                    }
-                    qt[7][m] = t;
+                const bool xin_a = j + 3 >= 4 && j + 3 < g.nx - 4;
+                switch (q & 7) {
+                    case 0: queue_phase<0>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 1: queue_phase<1>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 2: queue_phase<2>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 3: queue_phase<3>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 4: queue_phase<4>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 5: queue_phase<5>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    case 6: queue_phase<6>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
+                    default: queue_phase<7>(qp, qt, g, xin_a, txmask, pn, bn, sx, pc); break;
                 }
             }
             if (j >= xbeg) {
-                const bool inner = tile_inner && j >= 4 && j < g.nx - 4;
-                if (inner) ext_stage<true>(g, j, z0, y0, st, TYs, TZs);
-                else ext_stage<false>(g, j, z0, y0, st, TYs, TZs);
+                const bool xin = j >= 4 && j < g.nx - 4;
+                // one code path for every tile (the selects are cheap, code size is not)
+                ext_stage<EDGE>(g, xin, tile_top, z0, y0, st, TYs, TZs);
                 __syncthreads();
-                if (own) {
-                    float sx[4], pc[4];
-#pragma unroll
-                    for (int m = 0; m < 4; m++) {
-                        sx[m] = st8(g, qt[0][m], qt[1][m], qt[2][m], qt[3][m], qt[4][m], qt[5][m], qt[6][m], qt[7][m]);
-                        pc[m] = qp[0][m];
-                    }
-                    if (inner) fin_stage<true>(g, j, z, y, zq, row, sx, pc, st, TYs, TZs, F.pold, F.pspace);
-                    else fin_stage<false>(g, j, z, y, zq, row, sx, pc, st, TYs, TZs, F.pold, F.pspace);
-                }
+                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, zq, row, sx, pc, st, TYs, TZs, F.pold, F.pspace);
             }
             __syncthreads();
             if (*abort_flag) {

@@ -5,7 +5,7 @@
 
 #include <string>
 
-#include "../../include/wavefd_b200.h"
+#include "wavefd_b200.h"
 #include "wfd_kernels.h"
 
 namespace wfd {

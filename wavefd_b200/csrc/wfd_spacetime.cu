@@ -17,7 +17,7 @@
 #include <numeric>
 #include <vector>
 
-#include "../../include/wavefd_b200.h"
+#include "wavefd_b200.h"
 #include "wfd_prop.h"
 
 namespace wfd {
