@@ -287,6 +287,20 @@ int WFD_Inject(void *table, float *field, const float *data, long it, long nt, v
 /* data[(ir-1)*nt + it-1] += c * field[iu-1] on the device */
 int WFD_Extract(void *table, float *data, const float *field, long it, long nt, void *stream);
 
+/* No counterpart in the reference. The wavefield-separation imaging condition (the arithmetic of
+ * AdjointBornAccumulation_wavefieldsep / _wavefieldsep_V) for callers that cannot call cudaMalloc:
+ * it allocates no memory. Every array must already be device or managed memory (nx*ny*nz floats,
+ * z fastest; ny = 1 for 2D; wavefieldDM and mOld both NULL for the isotropic case); dVel is
+ * accumulated. Its FFT scratch is a fixed 160 KiB device array inside the library, so nz is
+ * limited to 2048 (larger nz returns WFD_ERR_ARG). The first call on each device looks up that
+ * array's device address; make that first call before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race. Work is enqueued on `stream` (a cudaStream_t, NULL
+ * for the default stream) without host synchronisation. Returns a WFD_* status. */
+int WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(long nx, long ny, long nz, long isFWI, const float *v,
+                                                     const float *b, const float *wavefieldDP, const float *pOld,
+                                                     const float *wavefieldDM, const float *mOld, float *dVel,
+                                                     void *stream);
+
 #ifdef __cplusplus
 }
 #endif

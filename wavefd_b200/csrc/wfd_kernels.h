@@ -64,6 +64,9 @@ struct Scratch {
     void image_wavefieldsep(const wfd::Grid &g, long isfwi, const wfd::Fields &F, const float *dp,       \
                             const float *dm, float *dv, float2 *work, long ncols_per_pass,               \
                             cudaStream_t s);                                                             \
+    void image_wavefieldsep_tables(const wfd::Grid &g, long isfwi, const wfd::Fields &F, const float *dp, \
+                                   const float *dm, float *dv, const float2 *tables, int m,              \
+                                   cudaStream_t s);                                                      \
     }
 
 WFD_DECLARE_LAUNCHERS(wfd_fast)

@@ -165,6 +165,29 @@ void host_fft(std::vector<double> &re, std::vector<double> &im, int sign) {
 
 }  // namespace
 
+// Launch with Bluestein tables already on the device ({chirp[n], filter(+1)[m], filter(-1)[m]},
+// m = 0 for power-of-two n); allocates nothing.
+void image_wavefieldsep_tables(const Grid &g, long isfwi, const Fields &F, const float *dp, const float *dm,
+                               float *dv, const float2 *tables, int m, cudaStream_t s) {
+    const int n = (int)(2 * g.nz);
+    SepTables T{nullptr, nullptr, nullptr, n, m};
+    if (m) {
+        T.chirp = tables;
+        T.vplus = tables + n;
+        T.vminus = tables + n + m;
+    }
+    const long nz = g.nz;
+    const size_t smem = sizeof(float2) * (size_t)n + sizeof(float2) * (size_t)nz +
+                        sizeof(float) * (size_t)(nz + (nz & 1)) + sizeof(float2) * (size_t)m;
+    cudaFuncSetAttribute(k_wavefieldsep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const long ncols = g.nx * g.ny;
+    const long chunk = 65535;
+    for (long c0 = 0; c0 < ncols; c0 += chunk) {
+        const long nb = ncols - c0 < chunk ? ncols - c0 : chunk;
+        k_wavefieldsep<<<(unsigned)nb, 256, smem, s>>>(g, isfwi, F, dp, dm, dv, T, c0);
+    }
+}
+
 void image_wavefieldsep(const Grid &g, long isfwi, const Fields &F, const float *dp, const float *dm, float *dv,
                         float2 *work, long ncols_per_pass, cudaStream_t s) {
     (void)work;
