@@ -43,6 +43,14 @@ WORKLOADS = {
                    nt=2000, nsponge=40, fpeak=12.0, nrec=(256, 256), bytes_per_cell=72,
                    label="3D AcoTTIDenQ forward, 400^3 (64M cells), 10 m, dt 0.5 ms, nt 2000, 40-cell sponge, "
                          "12 Hz Ricker, 256x256 surface receivers"),
+    "vti400": dict(physics="vti", name="Prop3DAcoVTIDenQ_DEO2_FDTD", shape=(400, 400, 400), d=10.0, dt=0.0005,
+                   nt=2000, nsponge=40, fpeak=12.0, nrec=(256, 256), bytes_per_cell=56,
+                   label="3D AcoVTIDenQ forward, 400^3 (64M cells), 10 m, dt 0.5 ms, nt 2000, 40-cell sponge, "
+                         "12 Hz Ricker, 256x256 surface receivers"),
+    # profiling-size case of the TTI kernel (fields still larger than L2: 67 MB each)
+    "tti256": dict(physics="tti", name="Prop3DAcoTTIDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
+                   nt=2000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=72,
+                   label="3D AcoTTIDenQ forward, 256^3 (16.8M cells), profiling size"),
 }
 METRIC = "Mcells/s & %HBM roofline, 3D Iso/TTI step; Born image s/shot learned vs plain"
 
@@ -232,7 +240,7 @@ def run_ours(args, W):
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     peak, peak_src = peaks()
     traffic = profiled_traffic(W["name"])
-    launches_per_step = 1 if prop.physics == "iso" else 2
+    launches_per_step = lib.WFD_Prop_StepKernels(prop.p)
     clocks = clk.summary()
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "Mcells/s", "n_gpus": world, "steps": K, "warmup": Wu,

@@ -277,6 +277,8 @@ int WFD_Prop_Synchronize(void *p);
 int WFD_Prop_Prefetch(void *p);
 /* the object's CUDA stream (a cudaStream_t) */
 void *WFD_Prop_Stream(void *p);
+/* kernels the last time step launched: 1 = fused single-sweep kernel, 2 = the two passes */
+int WFD_Prop_StepKernels(void *p);
 /* device-resident source/receiver tables built from a flat point list (grouped by written
  * location, contributions accumulated in list order, as the reference does partition-wise) */
 void *WFD_Points_Create(const SourcePoint32 *points, long npoints, int by_receiver);

@@ -22,8 +22,9 @@ NAMES = list(PROPAGATORS)
 FAST_TOL = 1e-5
 
 # odd sizes: partial tiles in z and y, and x split into several fused-kernel chunks; nz = 37 takes
-# the fused kernel that stages tiles with ordinary loads, nz = 36 the TMA-staged one
-ODD_SHAPES = {2: [(45, 1, 150)], 3: [(37, 21, 140), (36, 21, 150)]}
+# the fused kernel that stages tiles with ordinary loads, nz = 36 the TMA-staged one; nz = 100,
+# ny = 53 gives tiles whose halo lies wholly inside the interior
+ODD_SHAPES = {2: [(45, 1, 150)], 3: [(37, 21, 140), (36, 21, 150), (100, 53, 60)]}
 
 
 @pytest.fixture(scope="module")
@@ -69,7 +70,7 @@ def test_step_strict_bitwise(lib, oracle, name, fs, fused):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("fs", [True, False])
-@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("which", [0, 1, 2])
 def test_step_strict_bitwise_odd_sizes(lib, oracle, name, fs, which):
     ndim = PROPAGATORS[name][0]
     if which >= len(ODD_SHAPES[ndim]):
@@ -90,6 +91,20 @@ def test_step_fast_close(lib, oracle, name, fs):
     for _ in range(40):
         gpu.abi.TimeStep(gpu.p)
         orc.step()
+    for k in _fields(name):
+        err = rel_l2(gpu.arr(k), orc.arr(k))
+        assert err <= FAST_TOL, f"{name} {k}: rel L2 {err:.3e}"
+    gpu.close()
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if PROPAGATORS[n][0] == 3])
+@pytest.mark.parametrize("fs", [True, False])
+def test_step_fast_close_interior_tiles(lib, oracle, name, fs):
+    gpu, orc = _pair(lib, oracle, name, fs, shape=ODD_SHAPES[3][2], seed=9, strict=False)
+    for _ in range(30):
+        gpu.abi.TimeStep(gpu.p)
+        orc.step()
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(gpu.p)) == 0
     for k in _fields(name):
         err = rel_l2(gpu.arr(k), orc.arr(k))
         assert err <= FAST_TOL, f"{name} {k}: rel L2 {err:.3e}"

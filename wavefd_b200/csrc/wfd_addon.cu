@@ -63,3 +63,5 @@ extern "C" int WFD_Prop_Prefetch(void *p) {
 }
 
 extern "C" void *WFD_Prop_Stream(void *p) { return p ? (void *)P(p)->stream : nullptr; }
+
+extern "C" int WFD_Prop_StepKernels(void *p) { return p ? P(p)->step_kernels : WFD_ERR_ARG; }

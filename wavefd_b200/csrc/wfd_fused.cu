@@ -5,14 +5,17 @@ namespace WFD_NS {
 using namespace wfd;
 
 bool fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
-    (void)linear;
     if (g.ndim == 3 && phys == ISO) {
         // TMA-staged kernel when the tensor maps can be encoded (nz*4 a multiple of 16 bytes),
         // else the variant that stages its tiles with ordinary loads
         if (fused_iso3d_tma(g, F, s)) return true;
         return fused_iso3d(g, F, s);
     }
+    if (g.ndim == 3 && (phys == VTI || phys == TTI)) return fused_aniso3d_tma(g, phys, linear, F, s);
     return false;
 }
+
+// timeout flags of every fused kernel, cleared on read
+unsigned fused_status_and_clear() { return iso3d_status_and_clear() | aniso3d_status_and_clear(); }
 
 }  // namespace WFD_NS

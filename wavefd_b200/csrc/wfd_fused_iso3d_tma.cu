@@ -417,7 +417,7 @@ bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
     return true;
 }
 
-unsigned fused_status_and_clear() {
+unsigned iso3d_status_and_clear() {
     unsigned v = 0, z = 0;
     cudaMemcpyFromSymbol(&v, d_status, sizeof(v));
     if (v) cudaMemcpyToSymbol(d_status, &z, sizeof(z));

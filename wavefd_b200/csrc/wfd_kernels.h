@@ -36,6 +36,9 @@ struct Scratch {
                 float *oy, float *oz, cudaStream_t s);                                                   \
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
+    bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
+    unsigned iso3d_status_and_clear();                                                                   \
+    unsigned aniso3d_status_and_clear();                                                                 \
     unsigned fused_status_and_clear();                                                                   \
     void dminus3(const wfd::Grid &g, const float *fx, const float *fy, const float *fz, float *ox,       \
                  float *oy, float *oz, cudaStream_t s);                                                  \

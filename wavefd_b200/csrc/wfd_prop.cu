@@ -294,6 +294,7 @@ int prop_step(Prop *p, bool linear, bool sync) {
             wfd_fast::pass2(g, p->phys, linear, F, S, p->stream);
         }
     }
+    p->step_kernels = done ? 1 : 2;
     if (int rc = check_cuda(p, cudaGetLastError(), "time step launch")) return rc;
     // pointer swap (prop3DAcoIsoDenQ_DEO2_FDTD.h:258-260)
     std::swap(p->field[F_PCUR], p->field[F_POLD]);

@@ -37,6 +37,7 @@ struct Prop {
     int status = WFD_OK;
     std::string message;
     long steps = 0;
+    int step_kernels = 0;  // kernels launched by the last time step (1 fused, 2 unfused)
 
     long ncells() const { return nx * ny * nz; }
     Grid grid() const;
