@@ -289,6 +289,45 @@ int WFD_Inject(void *table, float *field, const float *data, long it, long nt, v
 /* data[(ir-1)*nt + it-1] += c * field[iu-1] on the device */
 int WFD_Extract(void *table, float *data, const float *field, long it, long nt, void *stream);
 
+/* Batched shots (no counterpart in the reference, whose Ginsu is exported but not defined,
+ * src/WaveFD.jl:52). A batch advances many 3D objects made by the *_alloc calls above (uneven sizes;
+ * Iso, VTI and TTI mixed; same dx, dy, dz, dt, free surface and strict/fast mode; nz a multiple of 4)
+ * with one persistent launch per physics class per time step; each object's arrays are bitwise
+ * those of stepping it alone, and its getters and pointer swap stay valid. The objects must outlive
+ * the batch. Returns NULL on error (WFD_LastError). */
+void *WFD_Batch_Create(void *const *props, long nprops);
+void WFD_Batch_Free(void *batch);
+int WFD_Batch_Status(void *batch);
+const char *WFD_Batch_Message(void *batch);
+/* Sources and receivers of shot i (its points, 1-based iu into that object's grid and ir into the
+ * traces) with device-resident wavelet and traces, column-major (nt, ntraces). Each step injects
+ * the wavelet at the current time index into pCur after the step, then extracts pCur into the
+ * traces, as WFD_Inject / WFD_Extract do; time indices beyond nt are skipped. nsrc = nrec = 0 clears. */
+int WFD_Batch_SetAcquisition(void *batch, long shot, const SourcePoint32 *src, long nsrc, const float *wavelet,
+                             const SourcePoint32 *rec, long nrec, float *traces, long nt);
+/* Explicit plan: x-chunk length target (the tiles' extent along the sweep; 0 = whole nx), item order
+ * (0 = longest first, 1 = shots interleaved), class launches concurrent (1) or serial (0). */
+int WFD_Batch_Plan(void *batch, long xchunk_target, int order, int concurrent);
+/* Autotune the plan by timing candidate launches (reps each) on the batch's own arrays; the arrays
+ * the trial launches overwrite are saved first and restored after (a temporary device copy). */
+int WFD_Batch_Tune(void *batch, int reps);
+/* Advance every shot nsteps time steps, injecting/extracting at time indices it0, it0+1, ...;
+ * use_graph != 0 replays a captured two-step CUDA graph. Asynchronous on the batch's stream, which
+ * is ordered after, and before, work on the objects' own streams. */
+int WFD_Batch_Run(void *batch, long nsteps, long it0, int use_graph);
+int WFD_Batch_Synchronize(void *batch);
+void *WFD_Batch_Stream(void *batch);
+/* info[0..15]: per class (Iso, VTI, TTI) {shots, items, CTAs, x-chunk target}; mode (0 concurrent);
+ * item orders (bit per class); kernels per step; tuned. */
+int WFD_Batch_Info(void *batch, long *info, long ninfo);
+/* Ginsu window of a survey array: shot[x,y,z] = survey[x0+x, y0+y, z0+z] (indices clamped to the
+ * survey), and the scatter-add of a shot image back into the survey image. Device arrays, (nz,ny,nx)
+ * z-fastest; asynchronous on `stream`. */
+int WFD_Ginsu_Crop(const float *survey, long snx, long sny, long snz, long x0, long y0, long z0, float *shot,
+                   long nx, long ny, long nz, void *stream);
+int WFD_Ginsu_Accumulate(float *survey, long snx, long sny, long snz, long x0, long y0, long z0, const float *shot,
+                         long nx, long ny, long nz, void *stream);
+
 /* No counterpart in the reference. The wavefield-separation imaging condition (the arithmetic of
  * AdjointBornAccumulation_wavefieldsep / _wavefieldsep_V) for callers that cannot call cudaMalloc:
  * it allocates no memory. Every array must already be device or managed memory (nx*ny*nz floats,

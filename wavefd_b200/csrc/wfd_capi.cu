@@ -24,16 +24,7 @@ thread_local bool t_host_touched = false;
 void before_device(Prop *p) {
     if (!t_host_touched) return;
     t_host_touched = false;
-    const size_t bytes = sizeof(float) * (size_t)p->ncells();
-    for (int f = 0; f < wfd::F_COUNT; f++) {
-        if (!p->field[f]) continue;
-#if CUDART_VERSION >= 13000
-        cudaMemLocation loc{cudaMemLocationTypeDevice, p->device};
-        cudaMemPrefetchAsync(p->field[f], bytes, loc, 0, p->stream);
-#else
-        cudaMemPrefetchAsync(p->field[f], bytes, p->device, p->stream);
-#endif
-    }
+    wfd::prefetch_to_device(p, p->stream);
 }
 
 float *getter(void *p, int f) {
@@ -42,6 +33,29 @@ float *getter(void *p, int f) {
 }
 
 }  // namespace
+
+namespace wfd {
+
+void prefetch_to_device(Prop *p, cudaStream_t s) {
+    const size_t bytes = sizeof(float) * (size_t)p->ncells();
+    for (int f = 0; f < F_COUNT; f++) {
+        if (!p->field[f]) continue;
+#if CUDART_VERSION >= 13000
+        cudaMemLocation loc{cudaMemLocationTypeDevice, p->device};
+        cudaMemPrefetchAsync(p->field[f], bytes, loc, 0, s);
+#else
+        cudaMemPrefetchAsync(p->field[f], bytes, p->device, s);
+#endif
+    }
+}
+
+bool take_host_touched() {
+    const bool t = t_host_touched;
+    t_host_touched = false;
+    return t;
+}
+
+}  // namespace wfd
 
 #define WFD_COMMON(NAME)                                                                                   \
     extern "C" void NAME##_free(void *p) { wfd::prop_destroy(P(p)); }                                     \

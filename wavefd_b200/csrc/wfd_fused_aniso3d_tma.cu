@@ -238,22 +238,21 @@ __device__ __forceinline__ void queue_phase(const Grid &g, float2 (&qx)[8][2], f
     hj[1] = qh[PH & 3][1];
 }
 
-template <int PHYS, bool LINEAR>
+// BATCH = false: one propagator object, tensor maps in the kernel parameters, static items.
+// BATCH = true: many shots; each item names its shot, whose sizes, output pointers and tensor maps
+// sit in a descriptor in global memory; CTAs take items from a shared counter.
+template <int PHYS, bool LINEAR, bool BATCH>
 __global__ void __launch_bounds__(NT, 1)
-    k_aniso3d_tma(Grid g, Fields F, const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mM,
-                  const __grid_constant__ CUtensorMap mB, const __grid_constant__ CUtensorMap mE,
-                  const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mF,
-                  const __grid_constant__ CUtensorMap mST, const __grid_constant__ CUtensorMap mCT,
-                  const __grid_constant__ CUtensorMap mSP, const __grid_constant__ CUtensorMap mCP,
-                  const __grid_constant__ CUtensorMap mPO, const __grid_constant__ CUtensorMap mMO,
-                  const __grid_constant__ CUtensorMap mV, const __grid_constant__ CUtensorMap mQ,
-                  const __grid_constant__ CUtensorMap mBC, int ntz, int nty, int nch, int xchunk) {
+    k_aniso3d_tma(Grid g0, Fields F, const __grid_constant__ AnisoMaps M, int ntz0, int nty0, int nch0, int xchunk0,
+                  const AnisoShotDesc *__restrict__ shots, const int *__restrict__ sel,
+                  const int2 *__restrict__ items, int nitems, int *counter) {
     extern __shared__ __align__(1024) float sm[];
     float *TYs = sm + OFF_TY;  // [2][TYR][TZ]: y outputs of P then M
     float *TZs = sm + OFF_TZ;  // [2][TY][TZW]: z outputs of P then M
     uint64_t *rbar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
     uint64_t *mbar = rbar + NR;
     int *abort_flag = reinterpret_cast<int *>(mbar + NM);
+    int *item_slot = abort_flag + 1;
     constexpr int nmat = PHYS == TTI ? 8 : 4;
 
     const int tid = threadIdx.x;
@@ -287,12 +286,46 @@ __global__ void __launch_bounds__(NT, 1)
         h_kind = 0;
     }
 
-    const long total = (long)ntz * nty * nch;
+    const long total = (long)ntz0 * nty0 * nch0;
     unsigned rseq = 0, mseq = 0;      // ring planes and stages of the items finished by this CTA
     unsigned r_issued = 0, m_issued = 0;  // issued by thread 0
     unsigned r_done = 0, m_done = 0;      // landed (waits that succeeded)
 
-    for (long w = blockIdx.x; w < total; w += gridDim.x) {
+    for (long wstat = blockIdx.x;; wstat += gridDim.x) {
+        Grid g = g0;
+        const CUtensorMap *maps = M.m;
+        float *out_pold = F.pold, *out_mold = F.mold, *out_pspace = F.pspace, *out_mspace = F.mspace;
+        int ntz = ntz0, nty = nty0, xchunk = xchunk0;
+        long w = wstat;
+        if (BATCH) {
+            if (tid == 0) *item_slot = atomicAdd(counter, 1);
+            __syncthreads();
+            const int wi = *item_slot;
+            __syncthreads();
+            if (wi >= nitems) break;
+            const int2 it = items[wi];
+            const AnisoShotDesc *d = shots + sel[it.x];
+            g.nx = d->nx;
+            g.ny = d->ny;
+            g.nz = d->nz;
+            g.sy = d->nz;
+            g.sx = (long)d->ny * d->nz;
+            g.n = g.nx * g.sx;
+            maps = d->m;
+            out_pold = d->pold;
+            out_mold = d->mold;
+            out_pspace = d->pspace;
+            out_mspace = d->mspace;
+            ntz = d->ntz;
+            nty = d->nty;
+            xchunk = d->xchunk;
+            w = it.y;
+        } else if (wstat >= total) {
+            break;
+        }
+        const CUtensorMap *mP = maps + 0, *mM = maps + 1, *mB = maps + 2, *mE = maps + 3, *mA = maps + 4,
+                          *mF = maps + 5, *mST = maps + 6, *mCT = maps + 7, *mSP = maps + 8, *mCP = maps + 9,
+                          *mPO = maps + 10, *mMO = maps + 11, *mV = maps + 12, *mQ = maps + 13, *mBC = maps + 14;
         const int tzi = (int)(w % ntz);
         const int tyi = (int)((w / ntz) % nty);
         const int chi = (int)(w / ((long)ntz * nty));
@@ -311,8 +344,8 @@ __global__ void __launch_bounds__(NT, 1)
             uint64_t *bar = &rbar[gidx % NR];
             float *s = sm + OFF_RING + (gidx % NR) * R_SLOT;
             mbar_expect_tx(bar, 4u * R_SLOT);
-            tma_load_3d(s, &mP, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
-            tma_load_3d(s + RBOX, &mM, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
+            tma_load_3d(s, mP, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
+            tma_load_3d(s + RBOX, mM, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
         };
         auto issue_stage = [&](int q, unsigned gidx) {
             uint64_t *bar = &mbar[gidx % NM];
@@ -320,21 +353,21 @@ __global__ void __launch_bounds__(NT, 1)
             float *c = s + NMAT * MBOX;
             mbar_expect_tx(bar, 4u * (nmat * MBOX + NCORE * CBOX));
             const int P = (int)(jstart + q + 3), j = (int)(jstart + q);
-            tma_load_3d(s + MT_B * MBOX, &mB, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_E * MBOX, &mE, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_A * MBOX, &mA, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_F * MBOX, &mF, bar, z0 - 4, y0 - 4, P);
+            tma_load_3d(s + MT_B * MBOX, mB, bar, z0 - 4, y0 - 4, P);
+            tma_load_3d(s + MT_E * MBOX, mE, bar, z0 - 4, y0 - 4, P);
+            tma_load_3d(s + MT_A * MBOX, mA, bar, z0 - 4, y0 - 4, P);
+            tma_load_3d(s + MT_F * MBOX, mF, bar, z0 - 4, y0 - 4, P);
             if (PHYS == TTI) {
-                tma_load_3d(s + MT_ST * MBOX, &mST, bar, z0 - 4, y0 - 4, P);
-                tma_load_3d(s + MT_CT * MBOX, &mCT, bar, z0 - 4, y0 - 4, P);
-                tma_load_3d(s + MT_SP * MBOX, &mSP, bar, z0 - 4, y0 - 4, P);
-                tma_load_3d(s + MT_CP * MBOX, &mCP, bar, z0 - 4, y0 - 4, P);
+                tma_load_3d(s + MT_ST * MBOX, mST, bar, z0 - 4, y0 - 4, P);
+                tma_load_3d(s + MT_CT * MBOX, mCT, bar, z0 - 4, y0 - 4, P);
+                tma_load_3d(s + MT_SP * MBOX, mSP, bar, z0 - 4, y0 - 4, P);
+                tma_load_3d(s + MT_CP * MBOX, mCP, bar, z0 - 4, y0 - 4, P);
             }
-            tma_load_3d(c + C_PO * CBOX, &mPO, bar, z0, y0, j);
-            tma_load_3d(c + C_MO * CBOX, &mMO, bar, z0, y0, j);
-            tma_load_3d(c + C_V * CBOX, &mV, bar, z0, y0, j);
-            tma_load_3d(c + C_Q * CBOX, &mQ, bar, z0, y0, j);
-            tma_load_3d(c + C_B * CBOX, &mBC, bar, z0, y0, j);
+            tma_load_3d(c + C_PO * CBOX, mPO, bar, z0, y0, j);
+            tma_load_3d(c + C_MO * CBOX, mMO, bar, z0, y0, j);
+            tma_load_3d(c + C_V * CBOX, mV, bar, z0, y0, j);
+            tma_load_3d(c + C_Q * CBOX, mQ, bar, z0, y0, j);
+            tma_load_3d(c + C_B * CBOX, mBC, bar, z0, y0, j);
         };
         // antisymmetric image p[-k] = -p[k] (k = 1..3) above the free surface, in one ring plane
         auto image_plane = [&](unsigned gidx) {
@@ -492,8 +525,8 @@ __global__ void __launch_bounds__(NT, 1)
                     const float2 po = ld2(cs + (f == 0 ? C_PO : C_MO) * CBOX + o);
                     const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc, po))), po);
                     const float2 np = add2(t, mul2(bc2(2.0f), pc));
-                    st2((f == 0 ? F.pold : F.mold) + k, ok ? np : po);
-                    if (!LINEAR) st2((f == 0 ? F.pspace : F.mspace) + k, ok ? L[f] : bc2(0.0f));
+                    st2((f == 0 ? out_pold : out_mold) + k, ok ? np : po);
+                    if (!LINEAR) st2((f == 0 ? out_pspace : out_mspace) + k, ok ? L[f] : bc2(0.0f));
                 }
             }
             __syncthreads();
@@ -509,28 +542,39 @@ __global__ void __launch_bounds__(NT, 1)
     }
 }
 
-template <int PHYS, bool LINEAR>
-bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
-    CUtensorMap m[15];
+bool aniso_maps(const Grid &g, int phys, const Fields &F, CUtensorMap *m) {
     const float *srcs[15] = {F.pcur, F.mcur, F.b, F.eps, F.eta, F.f, F.st, F.ct, F.sp, F.cp,
                              F.pold, F.mold, F.v, F.q, F.b};
     for (int i = 0; i < 15; i++) {
         const float *src = srcs[i];
-        if (PHYS != TTI && i >= 6 && i <= 9) src = F.b;  // unused by VTI: any valid map
+        if (phys != TTI && i >= 6 && i <= 9) src = F.b;  // unused by VTI: any valid map
         unsigned bz = i < 2 ? RZW : (i < 10 ? MZW : TZ);
         unsigned by = i < 2 ? RYH : (i < 10 ? MYH : TY);
         if (!make_tensor_map_3d(&m[i], src, g.nx, g.ny, g.nz, bz, by, 1)) return false;
     }
-    auto kern = k_aniso3d_tma<PHYS, LINEAR>;
-    static int grid_cap = 0;
-    if (!grid_cap) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+    return true;
+}
+
+template <int PHYS, bool LINEAR>
+int aniso_grid_cap() {
+    static int cap = 0;
+    if (!cap) {
+        for (auto kern : {k_aniso3d_tma<PHYS, LINEAR, false>, k_aniso3d_tma<PHYS, LINEAR, true>})
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, NT, SMEM_BYTES);
-        grid_cap = sms * (per > 0 ? per : 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_aniso3d_tma<PHYS, LINEAR, false>, NT, SMEM_BYTES);
+        cap = sms * (per > 0 ? per : 1);
     }
+    return cap;
+}
+
+template <int PHYS, bool LINEAR>
+bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
+    AnisoMaps M;
+    if (!aniso_maps(g, PHYS, F, M.m)) return false;
+    const int grid_cap = aniso_grid_cap<PHYS, LINEAR>();
     const int ntz = (int)((g.nz + TZ - 1) / TZ);
     const int nty = (int)((g.ny + TY - 1) / TY);
     const long tiles = (long)ntz * nty;
@@ -550,8 +594,8 @@ bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
     const int nch = (int)((g.nx + xchunk - 1) / xchunk);
     const long work = tiles * nch;
     const int grid = (int)(work < grid_cap ? work : grid_cap);
-    kern<<<grid, NT, SMEM_BYTES, s>>>(g, F, m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8], m[9], m[10], m[11],
-                                      m[12], m[13], m[14], ntz, nty, nch, xchunk);
+    k_aniso3d_tma<PHYS, LINEAR, false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr,
+                                                                    nullptr, 0, nullptr);
     return true;
 }
 
@@ -562,6 +606,43 @@ bool fused_aniso3d_tma(const Grid &g, int phys, int linear, const Fields &F, cud
     if (phys == TTI) return linear ? false : launch<TTI, false>(g, F, s);
     if (phys == VTI) return linear ? launch<VTI, true>(g, F, s) : launch<VTI, false>(g, F, s);
     return false;
+}
+
+bool aniso3d_tma_describe(const Grid &g, int phys, const Fields &F, int xchunk, AnisoShotDesc *d, TileInfo *t) {
+    if (g.ndim != 3 || g.nz % 4 != 0 || xchunk < 1 || (phys != VTI && phys != TTI)) return false;
+    if (d) {
+        if (!aniso_maps(g, phys, F, d->m)) return false;
+        d->pold = F.pold;
+        d->mold = F.mold;
+        d->pspace = F.pspace;
+        d->mspace = F.mspace;
+        d->nx = (int)g.nx;
+        d->ny = (int)g.ny;
+        d->nz = (int)g.nz;
+        d->ntz = (int)((g.nz + TZ - 1) / TZ);
+        d->nty = (int)((g.ny + TY - 1) / TY);
+        d->xchunk = xchunk;
+    }
+    if (t) {
+        t->tz = TZ;
+        t->ty = TY;
+        t->warmup = WARMUP;
+        t->grid_cap = phys == TTI ? aniso_grid_cap<TTI, false>() : aniso_grid_cap<VTI, false>();
+    }
+    return true;
+}
+
+void aniso3d_tma_batch(const Grid &gc, int phys, const AnisoShotDesc *shots, const int *sel, const int2 *items,
+                       int nitems, int *counter, int grid, cudaStream_t s) {
+    if (phys == TTI) {
+        aniso_grid_cap<TTI, false>();
+        k_aniso3d_tma<TTI, false, true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, AnisoMaps{}, 0, 0, 0, 1, shots,
+                                                                     sel, items, nitems, counter);
+    } else {
+        aniso_grid_cap<VTI, false>();
+        k_aniso3d_tma<VTI, false, true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, AnisoMaps{}, 0, 0, 0, 1, shots,
+                                                                     sel, items, nitems, counter);
+    }
 }
 
 unsigned aniso3d_status_and_clear() {

@@ -237,16 +237,22 @@ __device__ __forceinline__ void queue_phase(float (&qp)[8][4], float (&qt)[8][4]
     }
 }
 
+// BATCH = false: one propagator object, its tensor maps in the kernel parameters, items w =
+// blockIdx.x, blockIdx.x + gridDim.x, ... of its (tile, x-chunk) list.
+// BATCH = true: many objects (shots) of different sizes; every item names its shot, whose sizes,
+// output pointers and tensor maps sit in a descriptor in global memory; CTAs take items from a
+// shared counter (dynamic scheduling over shots of uneven size, in the order the caller packed).
+template <bool BATCH>
 __global__ void __launch_bounds__(NT, 3)
-    k_iso3d_tma(Grid g, Fields F, const __grid_constant__ CUtensorMap mPH, const __grid_constant__ CUtensorMap mPN,
-                const __grid_constant__ CUtensorMap mBH, const __grid_constant__ CUtensorMap mBN,
-                const __grid_constant__ CUtensorMap mPO, const __grid_constant__ CUtensorMap mV,
-                const __grid_constant__ CUtensorMap mQ, int ntz, int nty, int nch, int xchunk) {
+    k_iso3d_tma(Grid g0, Fields F, const __grid_constant__ IsoMaps M, int ntz0, int nty0, int nch0, int xchunk0,
+                const IsoShotDesc *__restrict__ shots, const int *__restrict__ sel, const int2 *__restrict__ items,
+                int nitems, int *counter) {
     extern __shared__ __align__(1024) float sm[];
     float *TYs = sm + OFF_TY;
     float *TZs = sm + OFF_TZ;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
     int *abort_flag = reinterpret_cast<int *>(bars + NS);
+    int *item_slot = abort_flag + 1;
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -254,24 +260,50 @@ __global__ void __launch_bounds__(NT, 3)
     if (tid == 0) {
         for (int s = 0; s < NS; s++) mbar_init(&bars[s], 1);
         fence_mbar_init();
-        prefetch_tensor_map(&mPH);
-        prefetch_tensor_map(&mPN);
-        prefetch_tensor_map(&mBH);
-        prefetch_tensor_map(&mBN);
-        prefetch_tensor_map(&mPO);
-        prefetch_tensor_map(&mV);
-        prefetch_tensor_map(&mQ);
+        if (!BATCH)
+            for (int i = 0; i < 7; i++) prefetch_tensor_map(&M.m[i]);
         *abort_flag = 0;
     }
     __syncthreads();
 
-    const long total = (long)ntz * nty * nch;
+    const long total = (long)ntz0 * nty0 * nch0;
     unsigned gseq = 0;                  // groups consumed so far by this CTA
     unsigned out_from = 0, out_to = 0;  // groups issued but not yet consumed (thread 0)
     const int zq = lane & 7;
     const int row = 4 * warp + (lane >> 3);
 
-    for (long w = blockIdx.x; w < total; w += gridDim.x) {
+    for (long wstat = blockIdx.x;; wstat += gridDim.x) {
+        Grid g = g0;
+        const CUtensorMap *maps = M.m;
+        float *out_pold = F.pold, *out_pspace = F.pspace;
+        int ntz = ntz0, nty = nty0, xchunk = xchunk0;
+        long w = wstat;
+        if (BATCH) {
+            if (tid == 0) *item_slot = atomicAdd(counter, 1);
+            __syncthreads();
+            const int wi = *item_slot;
+            __syncthreads();
+            if (wi >= nitems) break;
+            const int2 it = items[wi];
+            const IsoShotDesc *d = shots + sel[it.x];
+            g.nx = d->nx;
+            g.ny = d->ny;
+            g.nz = d->nz;
+            g.sy = d->nz;
+            g.sx = (long)d->ny * d->nz;
+            g.n = g.nx * g.sx;
+            maps = d->m;
+            out_pold = d->pold;
+            out_pspace = d->pspace;
+            ntz = d->ntz;
+            nty = d->nty;
+            xchunk = d->xchunk;
+            w = it.y;
+        } else if (wstat >= total) {
+            break;
+        }
+        const CUtensorMap *mPH = maps + 0, *mPN = maps + 1, *mBH = maps + 2, *mBN = maps + 3, *mPO = maps + 4,
+                          *mV = maps + 5, *mQ = maps + 6;
         const int tzi = (int)(w % ntz);
         const int tyi = (int)((w / ntz) % nty);
         const int chi = (int)(w / ((long)ntz * nty));
@@ -296,13 +328,13 @@ __global__ void __launch_bounds__(NT, 3)
             uint64_t *bar = &bars[gs % NS];
             float *s = sm + (gs % NS) * STAGE;
             mbar_expect_tx(bar, GROUP_BYTES);
-            tma_load_3d(s + S_PH, &mPH, bar, z0 - 8, y0 - 7, (int)jj);
-            tma_load_3d(s + S_BH, &mBH, bar, z0 - 4, y0 - 4, (int)jj);
-            tma_load_3d(s + S_PN, &mPN, bar, z0, y0, (int)(jj + 7));
-            tma_load_3d(s + S_BN, &mBN, bar, z0, y0, (int)(jj + 3));
-            tma_load_3d(s + S_PO, &mPO, bar, z0, y0, (int)jj);
-            tma_load_3d(s + S_V, &mV, bar, z0, y0, (int)jj);
-            tma_load_3d(s + S_Q, &mQ, bar, z0, y0, (int)jj);
+            tma_load_3d(s + S_PH, mPH, bar, z0 - 8, y0 - 7, (int)jj);
+            tma_load_3d(s + S_BH, mBH, bar, z0 - 4, y0 - 4, (int)jj);
+            tma_load_3d(s + S_PN, mPN, bar, z0, y0, (int)(jj + 7));
+            tma_load_3d(s + S_BN, mBN, bar, z0, y0, (int)(jj + 3));
+            tma_load_3d(s + S_PO, mPO, bar, z0, y0, (int)jj);
+            tma_load_3d(s + S_V, mV, bar, z0, y0, (int)jj);
+            tma_load_3d(s + S_Q, mQ, bar, z0, y0, (int)jj);
         };
         if (tid == 0) {
             for (int q = 0; q < D && q < ngroups; q++) issue(jstart + q, gseq + q);
@@ -355,7 +387,8 @@ __global__ void __launch_bounds__(NT, 3)
                 // one code path for every tile (the selects are cheap, code size is not)
                 ext_stage<EDGE>(g, xin, tile_top, z0, y0, st, TYs, TZs);
                 __syncthreads();
-                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, zq, row, sx, pc, st, TYs, TZs, F.pold, F.pspace);
+                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, zq, row, sx, pc, st, TYs, TZs, out_pold,
+                                          out_pspace);
             }
             __syncthreads();
             if (*abort_flag) {
@@ -374,25 +407,39 @@ __global__ void __launch_bounds__(NT, 3)
 
 }  // namespace
 
-bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
-    if (g.nz % 4 != 0) return false;
-    CUtensorMap mPH, mPN, mBH, mBN, mPO, mV, mQ;
-    if (!make_tensor_map_3d(&mPH, F.pcur, g.nx, g.ny, g.nz, PZW, PYH, 1)) return false;
-    if (!make_tensor_map_3d(&mPN, F.pcur, g.nx, g.ny, g.nz, TZ, TY, 1)) return false;
-    if (!make_tensor_map_3d(&mBH, F.b, g.nx, g.ny, g.nz, BZW, BYH, 1)) return false;
-    if (!make_tensor_map_3d(&mBN, F.b, g.nx, g.ny, g.nz, TZ, TY, 1)) return false;
-    if (!make_tensor_map_3d(&mPO, F.pold, g.nx, g.ny, g.nz, TZ, TY, 1)) return false;
-    if (!make_tensor_map_3d(&mV, F.v, g.nx, g.ny, g.nz, TZ, TY, 1)) return false;
-    if (!make_tensor_map_3d(&mQ, F.q, g.nx, g.ny, g.nz, TZ, TY, 1)) return false;
-    static int grid_cap = 0;
-    if (!grid_cap) {
-        cudaFuncSetAttribute(k_iso3d_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+namespace {
+
+int iso_grid_cap() {
+    static int cap = 0;
+    if (!cap) {
         int dev = 0, sms = 0, per = 0;
+        for (auto kern : {k_iso3d_tma<false>, k_iso3d_tma<true>})
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_iso3d_tma, NT, SMEM_BYTES);
-        grid_cap = sms * (per > 0 ? per : 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_iso3d_tma<false>, NT, SMEM_BYTES);
+        cap = sms * (per > 0 ? per : 1);
     }
+    return cap;
+}
+
+bool iso_maps(const Grid &g, const Fields &F, CUtensorMap *m) {
+    return make_tensor_map_3d(&m[0], F.pcur, g.nx, g.ny, g.nz, PZW, PYH, 1) &&
+           make_tensor_map_3d(&m[1], F.pcur, g.nx, g.ny, g.nz, TZ, TY, 1) &&
+           make_tensor_map_3d(&m[2], F.b, g.nx, g.ny, g.nz, BZW, BYH, 1) &&
+           make_tensor_map_3d(&m[3], F.b, g.nx, g.ny, g.nz, TZ, TY, 1) &&
+           make_tensor_map_3d(&m[4], F.pold, g.nx, g.ny, g.nz, TZ, TY, 1) &&
+           make_tensor_map_3d(&m[5], F.v, g.nx, g.ny, g.nz, TZ, TY, 1) &&
+           make_tensor_map_3d(&m[6], F.q, g.nx, g.ny, g.nz, TZ, TY, 1);
+}
+
+}  // namespace
+
+bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
+    if (g.nz % 4 != 0) return false;
+    IsoMaps M;
+    if (!iso_maps(g, F, M.m)) return false;
+    const int grid_cap = iso_grid_cap();
     const int ntz = (int)((g.nz + TZ - 1) / TZ);
     const int nty = (int)((g.ny + TY - 1) / TY);
     // x-chunking: balance the last wave of persistent CTAs against the warm-up planes per chunk
@@ -413,8 +460,37 @@ bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
     const int nch = (int)((g.nx + xchunk - 1) / xchunk);
     const long work = tiles * nch;
     const int grid = (int)(work < grid_cap ? work : grid_cap);
-    k_iso3d_tma<<<grid, NT, SMEM_BYTES, s>>>(g, F, mPH, mPN, mBH, mBN, mPO, mV, mQ, ntz, nty, nch, xchunk);
+    k_iso3d_tma<false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr, 0,
+                                                    nullptr);
     return true;
+}
+
+bool iso3d_tma_describe(const Grid &g, const Fields &F, int xchunk, IsoShotDesc *d, TileInfo *t) {
+    if (g.ndim != 3 || g.nz % 4 != 0 || xchunk < 1) return false;
+    if (d) {
+        if (!iso_maps(g, F, d->m)) return false;
+        d->pold = F.pold;
+        d->pspace = F.pspace;
+        d->nx = (int)g.nx;
+        d->ny = (int)g.ny;
+        d->nz = (int)g.nz;
+        d->ntz = (int)((g.nz + TZ - 1) / TZ);
+        d->nty = (int)((g.ny + TY - 1) / TY);
+        d->xchunk = xchunk;
+    }
+    if (t) {
+        t->tz = TZ;
+        t->ty = TY;
+        t->warmup = WARMUP;
+        t->grid_cap = iso_grid_cap();
+    }
+    return true;
+}
+
+void iso3d_tma_batch(const Grid &gc, const IsoShotDesc *shots, const int *sel, const int2 *items, int nitems,
+                     int *counter, int grid, cudaStream_t s) {
+    k_iso3d_tma<true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, IsoMaps{}, 0, 0, 0, 1, shots, sel, items, nitems,
+                                                   counter);
 }
 
 unsigned iso3d_status_and_clear() {

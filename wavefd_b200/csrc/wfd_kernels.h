@@ -3,6 +3,7 @@
 // wfd_fast (FMA contraction, approximate division) per propagator object.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "wfd_common.cuh"
@@ -18,6 +19,35 @@ struct Fields {
 // Scratch of the unfused passes (the reference's tmp arrays), device memory.
 struct Scratch {
     float *t[12];
+};
+
+// Tensor maps of the TMA step kernels, passed by value (single object) or held in a shot descriptor.
+struct IsoMaps {
+    CUtensorMap m[7];  // pCur halo box, pCur tile, B halo box, B tile, pOld, V, Q
+};
+struct AnisoMaps {
+    CUtensorMap m[15];  // pCur, mCur (ring boxes), b, eps, eta, f, st, ct, sp, cp (halo boxes), pOld, mOld, V, Q, b
+};
+
+// One shot of a batched launch (device memory, read by the kernel per work item): its sizes, the
+// arrays the kernel stores to, its tensor maps and its x-chunk length. A work item is (shot,
+// local item) with local item = (chunk * nty + tile_y) * ntz + tile_z.
+struct alignas(64) IsoShotDesc {
+    CUtensorMap m[7];
+    float *pold, *pspace;
+    int nx, ny, nz, ntz, nty, xchunk;
+};
+struct alignas(64) AnisoShotDesc {
+    CUtensorMap m[15];
+    float *pold, *mold, *pspace, *mspace;
+    int nx, ny, nz, ntz, nty, xchunk;
+};
+
+// Tile geometry and capacity of a TMA step kernel, for the batch planner.
+struct TileInfo {
+    int tz, ty;      // (z, y) cross-section of a tile
+    int warmup;      // planes swept before the first output plane of an x-chunk
+    int grid_cap;    // resident CTAs on this device (SMs x CTAs per SM)
 };
 
 }  // namespace wfd
@@ -38,6 +68,16 @@ struct Scratch {
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     unsigned iso3d_status_and_clear();                                                                   \
+    /* batched launches over many shots (descriptors and items in device memory) */                     \
+    bool iso3d_tma_describe(const wfd::Grid &g, const wfd::Fields &F, int xchunk, wfd::IsoShotDesc *d,   \
+                            wfd::TileInfo *t);                                                           \
+    void iso3d_tma_batch(const wfd::Grid &gc, const wfd::IsoShotDesc *shots, const int *sel,            \
+                         const int2 *items, int nitems, int *counter, int grid, cudaStream_t s);        \
+    bool aniso3d_tma_describe(const wfd::Grid &g, int phys, const wfd::Fields &F, int xchunk,           \
+                              wfd::AnisoShotDesc *d, wfd::TileInfo *t);                                  \
+    void aniso3d_tma_batch(const wfd::Grid &gc, int phys, const wfd::AnisoShotDesc *shots,              \
+                           const int *sel, const int2 *items, int nitems, int *counter, int grid,       \
+                           cudaStream_t s);                                                              \
     unsigned aniso3d_status_and_clear();                                                                 \
     unsigned fused_status_and_clear();                                                                   \
     void dminus3(const wfd::Grid &g, const float *fx, const float *fy, const float *fz, float *ox,       \

@@ -65,6 +65,12 @@ int global_error(std::string *msg);
 void apply_dplus2d(bool fs, long nx, long nz, float c1, float c2, float c3, float c4, float invDx, float invDz,
                    const float *inX, const float *inZ, float *outX, float *outZ);
 
+// move every array of the object to its device (managed memory written by host code through the
+// getters); take_host_touched() reports, and clears, whether a getter was called since the last
+// device call on this thread
+void prefetch_to_device(Prop *p, cudaStream_t s);
+bool take_host_touched();
+
 // true when the pointer can be dereferenced by kernels (device or managed memory)
 bool device_accessible(const void *ptr);
 
