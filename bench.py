@@ -51,6 +51,13 @@ WORKLOADS = {
     "tti256": dict(physics="tti", name="Prop3DAcoTTIDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
                    nt=2000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=72,
                    label="3D AcoTTIDenQ forward, 256^3 (16.8M cells), profiling size"),
+    # batched shots: 64 ginsu windows of a 1024 x 1024 x 400 survey, apertures U{160..320} per axis,
+    # depth 400, Iso/VTI 50/50 by seed, one persistent launch per physics class, CUDA-graph time loop
+    "batch64": dict(physics="mixed", name="batch", survey=(1024, 1024, 400), nshots=64, aperture=(160, 320),
+                    d=10.0, dt=0.0005, nt=1500, nsponge=40, fpeak=12.0, nrec=(32, 32),
+                    label="batched 3D AcoIso/VTI DenQ forward: 64 ginsu windows (160-320)^2 x 400 of a "
+                          "1024x1024x400 survey, Iso/VTI 50/50, nt 1500, one persistent launch per physics "
+                          "class, CUDA-graph time loop, autotuned plan"),
 }
 METRIC = "Mcells/s & %HBM roofline, 3D Iso/TTI step; Born image s/shot learned vs plain"
 
@@ -272,6 +279,162 @@ def run_ours(args, W):
         print(json.dumps(out), flush=True)
 
 
+def batch_layout(W):
+    """The shot windows of the batched workload: (physics, (nx, ny, nz), (x0, y0)) per shot, seeded."""
+    rng = np.random.default_rng(3)
+    snx, sny, snz = W["survey"]
+    lo, hi = W["aperture"]
+    shots = []
+    for _ in range(W["nshots"]):
+        nx, ny = (int(v) for v in rng.integers(lo, hi + 1, 2))
+        phys = "iso" if rng.random() < 0.5 else "vti"
+        x0 = int(rng.integers(0, snx - nx + 1))
+        y0 = int(rng.integers(0, sny - ny + 1))
+        shots.append((phys, (nx, ny, snz), (x0, y0)))
+    return shots
+
+
+def run_batch(args, W):
+    import torch
+
+    from wavefd_b200 import _lib, props, synthetic
+    from wavefd_b200.batch import ShotBatch, ginsu_crop
+    from wavefd_b200.spacetime import causal_ricker
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    _lib.library()
+    nt = W["nt"]
+    layout = batch_layout(W)
+    survey = synthetic.earth_model(W["survey"], "vti", seed=3 + rank, d=W["d"], dt=W["dt"], nsponge=W["nsponge"],
+                                   q_blocks=False, device="cuda")
+    shots, srcs, recs, wavs, trcs = [], [], [], [], []
+    wav = torch.from_numpy(causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"]).astype(np.float32))
+    for phys, (nx, ny, nz), (x0, y0) in layout:
+        cls = props.Prop3DAcoIsoDenQ_DEO2_FDTD if phys == "iso" else props.Prop3DAcoVTIDenQ_DEO2_FDTD
+        p = cls(nz=nz, ny=ny, nx=nx, nsponge=W["nsponge"], dz=W["d"], dy=W["d"], dx=W["d"], dt=W["dt"],
+                freesurface=True, freqQ=5.0, qMin=0.1, qInterior=100.0)
+        names = ["V", "B"] + (["Eps", "Eta", "F"] if phys == "vti" else [])
+        for k in names:
+            dst = _managed_tensor(p, k, (nx, ny, nz))
+            ginsu_crop(survey[k], W["survey"], (x0, y0, 0), dst, (nx, ny, nz))
+        shots.append(p)
+        srcs.append(synthetic.center_source((nx, ny, nz), W["d"]))
+        recs.append(synthetic.surface_receivers((nx, ny, nz), W["nrec"][0], W["nrec"][1], W["nsponge"]))
+        wavs.append(wav.cuda())
+        trcs.append(torch.zeros(len(recs[-1]) * nt, device="cuda"))
+    del survey
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    for p in shots:
+        p.prefetch()
+    batch = ShotBatch(shots)
+    for i in range(len(shots)):
+        batch.set_acquisition(i, srcs[i], wavs[i], recs[i], trcs[i], nt)
+    torch.cuda.synchronize()
+    t_tune = time.perf_counter()
+    batch.tune(reps=2)
+    t_tune = time.perf_counter() - t_tune
+    info = batch.info()
+    stream = torch.cuda.ExternalStream(batch.stream())
+    cells = sum(nx * ny * nz for _, (nx, ny, nz), _ in layout)
+    alg = sum(nx * ny * nz * (28 if ph == "iso" else 56) for ph, (nx, ny, nz), _ in layout)
+    K, Wu = args.steps, args.warmup
+    if K % 2:
+        K += 1  # whole graph replays
+    batch.run(Wu, it0=1)
+    batch.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        batch.run(K, it0=Wu + 1, graph=True)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    batch.synchronize()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * cells * K / (ms / 1e3) / 1e6
+    # end to end: every step pair, the pair's source samples go up from pinned host memory into the
+    # shots' wavelets and the pair's receiver samples come back to pinned host memory
+    h_wav = wav.clone().pin_memory()
+    h_rec = [torch.empty((len(r), 2), pin_memory=True) for r in recs]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    it = Wu + K + 1
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    with torch.cuda.stream(stream):
+        for _ in range(K // 2):
+            for i in range(len(shots)):
+                wavs[i][it - 1:it + 1].copy_(h_wav[it - 1:it + 1], non_blocking=True)
+                h2d += 8
+            batch.run(2, it0=it, graph=True)
+            for i in range(len(shots)):
+                nr = len(recs[i])
+                h_rec[i].copy_(trcs[i].view(nr, nt)[:, it - 1:it + 1], non_blocking=True)
+                d2h += 8 * nr
+            it += 2
+            stream.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = world * cells * K / t_e2e / 1e6
+    peak, peak_src = peaks()
+    achieved = alg / (ms / K / 1e3) / 1e9
+    niso = sum(1 for ph, _, _ in layout if ph == "iso")
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "Mcells/s", "n_gpus": world, "steps": K, "warmup": Wu,
+        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded layered+random survey model, Gardner density, ginsu windows)",
+        "config": {"workload": W["label"], "survey": list(W["survey"]), "shots": len(layout), "iso_shots": niso,
+                   "vti_shots": len(layout) - niso, "cells_per_step": cells, "time_steps_per_shot": nt,
+                   "l2": "inputs larger than L2 (about 50 GB of shot arrays)", "parallelism": f"shots x{world}",
+                   "plan": info, "tune_s": round(t_tune, 2)},
+        "e2e": {"value": round(e2e, 1), "unit": "Mcells/s", "h2d_bytes_per_step": h2d // K,
+                "d2h_bytes_per_step": d2h // K},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": "batched step launches (Iso and VTI classes) + injection/extraction, per step",
+                     "algorithmic_bytes_per_cell": "28 Iso, 56 VTI", "kernel_ms": round(ms / K, 4),
+                     "peak_source": peak_src},
+        "gpu_launches": K * info["kernels_per_step"],
+        "clocks": clk.summary(),
+    }
+    # tensors used on the batch's stream (device and pinned host memory) go before the stream does
+    del wavs, trcs, h_wav, h_rec
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    batch.free()
+    for p in shots:
+        props.free(p)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_batch(W, layout)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def _managed_tensor(prop, getter, shape):
     import torch
     ptr = ctypes.cast(getattr(prop.abi, "get" + getter)(prop.p), ctypes.c_void_p).value
@@ -374,12 +537,66 @@ def cpu_baseline(W):
                       f"{th} OpenMP threads, reference built with -O3 -ffast-math ({fl})"}
 
 
+def _batch_sample_ws(W, layout):
+    """Reference sample shots of the batched workload: one Iso and one VTI window of the mean size."""
+    ws = {}
+    n = len(layout)
+    mx = int(round(sum(s[1][0] for s in layout) / n)) // 4 * 4
+    my = int(round(sum(s[1][1] for s in layout) / n)) // 4 * 4
+    for ph, name in (("iso", "Prop3DAcoIsoDenQ_DEO2_FDTD"), ("vti", "Prop3DAcoVTIDenQ_DEO2_FDTD")):
+        ws[ph] = dict(W, physics=ph, name=name, shape=(mx, my, W["survey"][2]))
+    return ws
+
+
+def _batch_cpu_rate(W, layout, steps, warmup, seconds):
+    """Mcells/s of the whole batch on the host cores: each physics timed on a mean-size sample shot,
+    the batch's cells per step divided by the time the two rates give."""
+    ws = _batch_sample_ws(W, layout)
+    rates, notes, th, fl = {}, [], None, None
+    for ph, w in ws.items():
+        r = _cpu_run(w, nsteps_max=steps, seconds=seconds, warmup=warmup)
+        if r is None:
+            return None
+        rates[ph], n, th, fl, _ = r
+        notes.append(f"{ph} {'x'.join(map(str, w['shape']))}: {rates[ph]:.1f} Mcells/s over {n} steps")
+    t = sum(nx * ny * nz / rates[ph] for ph, (nx, ny, nz), _ in layout)
+    cells = sum(nx * ny * nz for _, (nx, ny, nz), _ in layout)
+    return cells / t, th, fl, "; ".join(notes)
+
+
+def cpu_baseline_batch(W, layout):
+    r = _batch_cpu_rate(W, layout, steps=10, warmup=1, seconds=10.0)
+    if r is None:
+        return {"value": None, "unit": "Mcells/s", "cores": None, "kind": "reference",
+                "sample": "reference library not built"}
+    v, th, fl, notes = r
+    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+            "sample": f"reference TimeStep + injectdata_float + extractdata_float on one mean-size Iso and one "
+                      f"VTI window ({notes}), median step times, combined over the batch's 64 windows; "
+                      f"{th} OpenMP threads, -O3 -ffast-math ({fl})"}
+
+
 def run_reference(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     if _ref_flavour() is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
+        return
+    if W["name"] == "batch":
+        layout = batch_layout(W)
+        v, th, fl, notes = _batch_cpu_rate(W, layout, steps=args.steps, warmup=args.warmup, seconds=60.0)
+        cells = sum(nx * ny * nz for _, (nx, ny, nz), _ in layout)
+        out = {
+            "metric": METRIC, "value": round(v, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(cells / v / 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": W["label"], "parallelism": f"OpenMP x{th}"},
+            "cpu_baseline": {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+                             "sample": notes},
+            "e2e": {"value": round(v, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(out), flush=True)
         return
     r = _cpu_run(W, nsteps_max=args.steps, seconds=1e9, warmup=args.warmup)
     v, n, th, fl, times = r
@@ -410,6 +627,8 @@ def main():
     W = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, W)
+    elif W["name"] == "batch":
+        run_batch(args, W)
     else:
         run_ours(args, W)
     # leave without running interpreter-teardown destructors (CUDA objects owned by two runtimes)
