@@ -328,6 +328,29 @@ int WFD_Ginsu_Crop(const float *survey, long snx, long sny, long snz, long x0, l
 int WFD_Ginsu_Accumulate(float *survey, long snx, long sny, long snz, long x0, long y0, long z0, const float *shot,
                          long nx, long ny, long nz, void *stream);
 
+/* Learned wavefield codec (no counterpart in the reference's arithmetic; it takes the role of
+ * CvxCompress in src/compressedio.jl:1-137, which compresses the saved forward fields). A 3D conv
+ * autoencoder (4^3/s4 1->16, 2^3/s2 16->32, and back), BF16 weights, FP32 accumulation: each 8^3
+ * block becomes 32 BF16 values and one FP32 scale. Device arrays, (nz,ny,nx) z-fastest; latent
+ * buffers hold WFD_Codec_LatentBytes bytes. Encode/decode are asynchronous on `stream`. */
+long WFD_Codec_NumParams(void);
+long WFD_Codec_LatentBytes(long nx, long ny, long nz);
+void *WFD_Codec_Create(unsigned seed);
+void WFD_Codec_Free(void *codec);
+/* FP32 master weights (host arrays of WFD_Codec_NumParams floats); SetWeights resets Adam's moments */
+int WFD_Codec_SetWeights(void *codec, const float *w, long n);
+int WFD_Codec_GetWeights(void *codec, float *w, long n);
+int WFD_Codec_Encode(void *codec, const float *field, long nx, long ny, long nz, void *latent, void *stream);
+int WFD_Codec_Decode(void *codec, const void *latent, long nx, long ny, long nz, float *field, void *stream);
+/* training: n 8^3 blocks at device origins[3*i..] (x, y, z) gathered in the codec's cell order and
+ * scaled by their max |value| (scales optional); one Adam step on a device batch of blocks
+ * (*loss, host, receives the batch's mean squared error before the step); the gradient of that
+ * loss without a step (host arrays grad[NumParams], *loss) */
+int WFD_Codec_GatherBlocks(const float *field, long nx, long ny, long nz, const int *origins, long n, float *blocks,
+                           float *scales, void *stream);
+int WFD_Codec_TrainStep(void *codec, const float *blocks, long n, float lr, float *loss, void *stream);
+int WFD_Codec_Gradient(void *codec, const float *blocks, long n, float *grad, float *loss);
+
 /* No counterpart in the reference. The wavefield-separation imaging condition (the arithmetic of
  * AdjointBornAccumulation_wavefieldsep / _wavefieldsep_V) for callers that cannot call cudaMalloc:
  * it allocates no memory. Every array must already be device or managed memory (nx*ny*nz floats,

@@ -1,0 +1,145 @@
+"""The learned wavefield codec on the GPU against its numpy restatement (oracle/codec_oracle.py):
+the training kernel's gradient, encode/decode of whole fields (the raw fallback blocks exact), and
+what training gains: the trained network against the untrained one and against the fixed-transform
+codec of the same size (3D DCT keeping 32 coefficients per 8^3 block, with the same raw fallback),
+on held-out propagated wavefields. Then the image of a Born shot with the codec storing the forward fields, against
+exact storage: relative L2 <= 1e-2."""
+import numpy as np
+import pytest
+
+from oracle import codec_oracle as co
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3
+IMAGE_TOL = 1e-2
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+def _smooth_blocks(torch, n, seed):
+    rng = np.random.default_rng(seed)
+    f = rng.standard_normal((40, 40, 40))
+    for ax in range(3):
+        for _ in range(3):
+            f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
+    B, _ = co.blocks_of(f.astype(np.float32))
+    B = B[:n]
+    B = B / np.abs(B).max(axis=1, keepdims=True)
+    return B.astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def trained(torch):
+    from wavefd_b200.codec import WavefieldCodec, train_on_propagated
+    codec = WavefieldCodec(seed=1)
+    init = codec.params.copy()
+    hist, nblocks = train_on_propagated(codec)
+    return codec, init, hist, nblocks
+
+
+def test_gradient_matches_oracle(torch):
+    from wavefd_b200.codec import WavefieldCodec
+    codec = WavefieldCodec(seed=3)
+    rng = np.random.default_rng(4)
+    w = codec.params + rng.standard_normal(co.NPARAM).astype(np.float32) * 0.02  # non-zero biases
+    codec.params = w
+    X = _smooth_blocks(torch, 96, 5)
+    g_gpu, loss_gpu = codec.gradient(torch.from_numpy(X).cuda())
+    g_ref = co.grad(codec.params, X)
+    l_ref = co.loss(codec.params, X)
+    assert abs(loss_gpu - l_ref) <= 1e-4 * l_ref
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    assert rel <= GRAD_TOL, rel
+    for name, (o, s) in co.OFFSETS.items():
+        n = int(np.prod(s))
+        r = np.linalg.norm(g_gpu[o:o + n] - g_ref[o:o + n]) / max(np.linalg.norm(g_ref[o:o + n]), 1e-30)
+        assert r <= 10 * GRAD_TOL, (name, r)
+
+
+def test_encode_decode_matches_oracle(torch):
+    from wavefd_b200.codec import WavefieldCodec
+    codec = WavefieldCodec(seed=7)
+    rng = np.random.default_rng(8)
+    for shape in [(40, 36, 72), (21, 30, 45)]:  # partial slabs; nz not a multiple of 4 in the second
+        f = rng.standard_normal(shape)
+        for ax in range(3):
+            f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
+        f = f.astype(np.float32) * np.float32(10.0) ** rng.uniform(-3, 3)
+        d_f = torch.from_numpy(f).cuda()
+        code = codec.empty_code(shape)
+        out = torch.empty(shape, device="cuda")
+        codec.encode(d_f, shape, code)
+        codec.decode(code, shape, out)
+        torch.cuda.synchronize()
+        g = out.cpu().numpy().astype(np.float64)
+        ref = co.roundtrip(codec.params, f)
+        B, _ = co.blocks_of(f)
+        nb = B.shape[0]
+        cap = max(1, nb // 100)
+        assert codec.raw_blocks(code, shape) == cap
+        Bg, _ = co.blocks_of(g.astype(np.float32))
+        Br, _ = co.blocks_of(ref.astype(np.float32))
+        raw = np.all(Bg == B, axis=1)  # blocks written back exactly
+        assert raw.sum() >= cap
+        keep = ~raw
+        rel = np.linalg.norm(Bg[keep] - Br[keep]) / np.linalg.norm(Br[keep])
+        assert rel <= 2e-3, rel
+        # the raw blocks are the worst-coded ones (up to the histogram's 1/8-octave bins)
+        err = ((Br.astype(np.float64) - B) ** 2).sum(1)
+        assert err[raw].min() >= np.sort(err)[-cap] / 2.0
+
+
+def test_training_reduces_loss(trained):
+    codec, init, hist, nblocks = trained
+    assert nblocks > 10000
+    assert np.mean(hist[-50:]) < 0.3 * np.mean(hist[:5])
+
+
+def test_trained_codec_gains_over_untrained_and_fixed_transform(torch, trained):
+    """Held-out wavefields (another seed): relative L2 error of the hybrid codec with the trained
+    weights, with the initial weights, and of the DCT codec of the same size."""
+    from wavefd_b200.codec import propagated_snapshots
+    codec, init, hist, _ = trained
+    snaps = propagated_snapshots((96, 96, 96), "tti", seed=99, nt=700, every=50)
+    trained_w = codec.params.copy()
+    errs = {"trained": [], "untrained": [], "dct32": []}
+    for f in snaps:
+        shape = tuple(f.shape)
+        code = codec.empty_code(shape)
+        out = torch.empty(shape, device="cuda")
+        fn = f.cpu().numpy()
+        for name, w in (("trained", trained_w), ("untrained", init)):
+            codec.params = w
+            codec.encode(f, shape, code)
+            codec.decode(code, shape, out)
+            torch.cuda.synchronize()
+            errs[name].append(np.linalg.norm(out.cpu().numpy() - fn) / np.linalg.norm(fn))
+        errs["dct32"].append(np.linalg.norm(co.dct_roundtrip(fn) - fn) / np.linalg.norm(fn))
+    codec.params = trained_w
+    m = {k: float(np.mean(v)) for k, v in errs.items()}
+    print("held-out relative L2 error:", m)
+    assert m["trained"] < 0.5 * m["untrained"]
+    assert m["trained"] < m["dct32"]
+
+
+def test_born_image_with_codec_matches_exact_storage(torch, trained):
+    from wavefd_b200 import imaging
+    codec = trained[0]
+    shot = imaging.make_shot("tti", (96, 96, 96), seed=5, nsponge=16, nt=600, nrec=(16, 16))
+    data = imaging.born_data(shot)
+    nsnap, nf = 600 // 4, 2
+    exact = imaging.DeviceStore(shot["shape"], nsnap, nf)
+    img_exact, _ = imaging.born_image(shot, data, exact, every=4)
+    store = imaging.CodecStore(codec, shot["shape"], nsnap, nf)
+    img_codec, _ = imaging.born_image(shot, data, store, every=4)
+    a, b = img_codec.cpu().numpy(), img_exact.cpu().numpy()
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    print(f"Born image relative L2, codec vs exact storage: {rel:.3e}; bytes {store.nbytes()} vs {exact.nbytes()}")
+    assert np.linalg.norm(b) > 0
+    assert rel <= IMAGE_TOL, rel
+    assert store.nbytes() * 15 < exact.nbytes()

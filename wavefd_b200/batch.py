@@ -60,6 +60,8 @@ def _addr(a):
     if a is None:
         return None
     if hasattr(a, "data_ptr"):
+        if hasattr(a, "is_contiguous") and not a.is_contiguous():
+            raise ValueError("the C ABI takes contiguous arrays (call .contiguous())")
         return c_void_p(a.data_ptr())
     if isinstance(a, int):
         return c_void_p(a)

@@ -1,0 +1,266 @@
+"""Born (linearised) imaging of one shot on the GPU, with the saved forward wavefield kept either in
+the learned codec's compressed form or uncompressed.
+
+This is the reference's workflow around the propagators (JetPackWaveFD drives WaveFD this way, and
+src/compressedio.jl:1-137 is its snapshot store): a forward run from the source saves the scaled
+spatial-derivative fields (pSpace, mSpace after ScaleSpatialDerivatives) every `every` steps; an
+adjoint run from the receivers back-propagates the recorded data and, at each saved step,
+accumulates the standard imaging condition (AdjointBornAccumulation_V) with the saved fields.
+
+Snapshot stores:
+  CodecStore   -- the learned codec (wfd_codec.cu), codes resident in device memory;
+  HostStore    -- uncompressed FP32 in pinned host memory, copies overlapped with the propagation
+                  (device staging ring + a copy stream, prefetch one snapshot ahead); the store for
+                  shots whose saved fields do not fit in device memory;
+  DeviceStore  -- uncompressed FP32 in device memory (exact reference for small shots).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import time
+
+import numpy as np
+
+from . import _lib, props, synthetic
+from .abi import SourcePoint32
+from .codec import _CAI
+
+_CLASSES = {"iso": props.Prop3DAcoIsoDenQ_DEO2_FDTD, "vti": props.Prop3DAcoVTIDenQ_DEO2_FDTD,
+            "tti": props.Prop3DAcoTTIDenQ_DEO2_FDTD}
+
+
+def _field(prop, name, shape):
+    import torch
+    ptr = ct.cast(getattr(prop.abi, "get" + name)(prop.p), ct.c_void_p).value
+    return torch.as_tensor(_CAI(ptr, shape), device="cuda")
+
+
+class DeviceStore:
+    def __init__(self, shape, nsnap, nfields):
+        import torch
+        self.buf = torch.empty((nsnap, nfields) + tuple(shape), device="cuda")
+
+    def put(self, k, fields, stream):
+        for i, f in enumerate(fields):
+            self.buf[k, i].copy_(f, non_blocking=True)
+
+    def get(self, k, stream):
+        return [self.buf[k, i] for i in range(self.buf.shape[1])]
+
+    def nbytes(self):
+        return self.buf.numel() * 4
+
+
+class CodecStore:
+    def __init__(self, codec, shape, nsnap, nfields):
+        import torch
+        self.codec, self.shape = codec, tuple(shape)
+        nb = codec.code_bytes(shape)
+        self.codes = torch.empty((nsnap, nfields, nb), dtype=torch.uint8, device="cuda")
+        self.out = [torch.empty(self.shape, device="cuda") for _ in range(nfields)]
+
+    def put(self, k, fields, stream):
+        for i, f in enumerate(fields):
+            self.codec.encode(f, self.shape, self.codes[k, i], stream)
+
+    def get(self, k, stream):
+        for i in range(len(self.out)):
+            self.codec.decode(self.codes[k, i], self.shape, self.out[i], stream)
+        return self.out
+
+    def nbytes(self):
+        return self.codes.numel()
+
+    def raw_blocks(self, k, i=0):
+        return self.codec.raw_blocks(self.codes[k, i], self.shape)
+
+
+class HostStore:
+    """Pinned host snapshots. A put copies the fields into a device staging slot on the propagation
+    stream (so the next time step may overwrite pSpace) and then to the host on a copy stream; a get
+    (the adjoint asks for snapshots in decreasing order) waits for its slot and starts the host-to-
+    device copy of the next one, so the copies overlap the propagation both ways."""
+
+    def __init__(self, shape, nsnap, nfields, ring=2):
+        import torch
+        self.shape, self.nf, self.ring = tuple(shape), nfields, ring
+        self.host = torch.empty((nsnap, nfields) + self.shape, pin_memory=True)
+        self.stage = torch.empty((ring, nfields) + self.shape, device="cuda")
+        self.copy = torch.cuda.Stream()
+        self.free_ev = [None] * ring   # the slot's last reader or copy is done after this event
+        self.ready_ev = [None] * ring  # the slot holds snapshot slot_k after this event
+        self.slot_k = [None] * ring
+
+    def put(self, k, fields, stream):
+        import torch
+        s = k % self.ring
+        if self.free_ev[s] is not None:
+            stream.wait_event(self.free_ev[s])
+        with torch.cuda.stream(stream):
+            for i, f in enumerate(fields):
+                self.stage[s, i].copy_(f, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.copy.wait_event(ev)
+        with torch.cuda.stream(self.copy):
+            self.host[k].copy_(self.stage[s], non_blocking=True)
+        fe = torch.cuda.Event()
+        fe.record(self.copy)
+        self.free_ev[s] = fe
+        self.slot_k[s] = None
+
+    def _fetch(self, k):
+        import torch
+        s = k % self.ring
+        if self.free_ev[s] is not None:
+            self.copy.wait_event(self.free_ev[s])
+        with torch.cuda.stream(self.copy):
+            self.stage[s].copy_(self.host[k], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(self.copy)
+        self.ready_ev[s] = ev
+        self.slot_k[s] = k
+
+    def get(self, k, stream):
+        s = k % self.ring
+        if self.slot_k[s] != k:
+            self._fetch(k)
+        stream.wait_event(self.ready_ev[s])
+        if k - 1 >= 0 and self.slot_k[(k - 1) % self.ring] != k - 1:
+            self._fetch(k - 1)
+        return [self.stage[s, i] for i in range(self.nf)]
+
+    def release(self, k, stream):
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.free_ev[k % self.ring] = ev
+
+    def nbytes(self):
+        return self.host.numel() * 4
+
+
+def make_shot(physics, shape, seed=0, d=10.0, dt=0.0005, nsponge=40, fpeak=12.0, nt=1000, nrec=(32, 32),
+              perturbation=True):
+    """Seeded shot: the earth model (device tensors), a Hicks source at the centre near the surface, a
+    surface receiver grid, the causal Ricker wavelet, and the Born velocity perturbation (+-2 % on 20
+    horizons, sparse) used as the reflectivity of the data."""
+    import torch
+    from .spacetime import causal_ricker
+    model = synthetic.earth_model(shape, physics, seed=seed, d=d, dt=dt, nsponge=nsponge, device="cuda")
+    src = synthetic.center_source(shape, d)
+    rec = synthetic.surface_receivers(shape, nrec[0], nrec[1], min(nsponge, shape[0] // 4))
+    wav = torch.from_numpy(causal_ricker(dt * np.arange(nt), f=fpeak).astype(np.float32)).cuda()
+    dv = None
+    if perturbation:
+        nx, ny, nz = shape
+        rng = np.random.default_rng(seed + 1000)
+        dv = torch.zeros(shape, device="cuda")
+        for z in np.linspace(nz * 0.15, nz * 0.9, 20).astype(int):
+            mask = torch.from_numpy((rng.random((nx, ny)) < 0.1).astype(np.float32)).cuda()
+            dv[:, :, z] = mask * model["V"][:, :, z] * float(rng.choice([-0.02, 0.02]))
+    return dict(model=model, src=src, rec=rec, wavelet=wav, dv=dv, shape=tuple(shape), d=d, dt=dt, nsponge=nsponge,
+                nt=nt, physics=physics)
+
+
+def _new_prop(shot):
+    nx, ny, nz = shot["shape"]
+    d = shot["d"]
+    p = _CLASSES[shot["physics"]](nz=nz, ny=ny, nx=nx, nsponge=shot["nsponge"], dz=d, dy=d, dx=d, dt=shot["dt"],
+                                  freesurface=True)
+    for k, t in shot["model"].items():
+        _field(p, k, shot["shape"]).copy_(t)
+    return p
+
+
+def born_data(shot):
+    """Linearised (Born) data of the shot's velocity perturbation at the receivers: the background
+    wavefield's scaled derivative field drives ForwardBornInjection_V into a second propagator."""
+    import torch
+    shape, nt = shot["shape"], shot["nt"]
+    lib = _lib.library()
+    p0, p1 = _new_prop(shot), _new_prop(shot)
+    torch.cuda.synchronize()
+    p0.prefetch()
+    p1.prefetch()
+    tsrc = lib.WFD_Points_Create(shot["src"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["src"]), 0)
+    trec = lib.WFD_Points_Create(shot["rec"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["rec"]), 1)
+    data = torch.zeros(len(shot["rec"]) * nt, device="cuda")
+    mtype = getattr(props, p1.NAME + "_Model_V")()
+    for it in range(1, nt + 1):
+        p0.step_async(1)
+        pc = ct.c_void_p(ct.cast(p0.abi.getPCur(p0.p), ct.c_void_p).value)
+        _lib.check(lib.WFD_Inject(tsrc, pc, ct.c_void_p(shot["wavelet"].data_ptr()), it, nt,
+                                  ct.c_void_p(p0.stream())), "inject")
+        p0.synchronize()
+        props.scale_spatial_derivatives(p0)
+        wf = {"pspace": _field(p0, "PSpace", shape)}
+        if shot["physics"] != "iso":
+            wf["mspace"] = _field(p0, "MSpace", shape)
+        props.propagateforward(p1)
+        props.forwardBornInjection(p1, mtype, {"v": shot["dv"]}, wf)
+        pc1 = ct.c_void_p(ct.cast(p1.abi.getPCur(p1.p), ct.c_void_p).value)
+        _lib.check(lib.WFD_Extract(trec, ct.c_void_p(data.data_ptr()), pc1, it, nt, ct.c_void_p(p1.stream())),
+                   "extract")
+        p1.synchronize()
+    lib.WFD_Points_Free(tsrc)
+    lib.WFD_Points_Free(trec)
+    props.free(p0)
+    props.free(p1)
+    return data
+
+
+def born_image(shot, data, store, every=4, nt=None):
+    """Adjoint Born image of the shot's data with the forward fields kept in `store`; returns
+    (image, seconds) with the forward and the adjoint run each timed on the device."""
+    import torch
+    shape = shot["shape"]
+    nt = nt or shot["nt"]
+    lib = _lib.library()
+    aniso = shot["physics"] != "iso"
+    fwd, adj = _new_prop(shot), _new_prop(shot)
+    torch.cuda.synchronize()
+    fwd.prefetch()
+    adj.prefetch()
+    tsrc = lib.WFD_Points_Create(shot["src"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["src"]), 0)
+    tadj = lib.WFD_Points_Create(shot["rec"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["rec"]), 0)
+    image = torch.zeros(shape, device="cuda")
+    mtype = getattr(props, adj.NAME + "_Model_V")()
+    ic = props.ImagingConditionStandard()
+    fs = torch.cuda.ExternalStream(fwd.stream())
+    as_ = torch.cuda.ExternalStream(adj.stream())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in range(1, nt + 1):
+        fwd.step_async(1)
+        pc = ct.c_void_p(ct.cast(fwd.abi.getPCur(fwd.p), ct.c_void_p).value)
+        _lib.check(lib.WFD_Inject(tsrc, pc, ct.c_void_p(shot["wavelet"].data_ptr()), it, shot["nt"],
+                                  ct.c_void_p(fwd.stream())), "inject")
+        if it % every == 0:
+            props.scale_spatial_derivatives(fwd)
+            f = [_field(fwd, "PSpace", shape)] + ([_field(fwd, "MSpace", shape)] if aniso else [])
+            store.put(it // every - 1, f, fs)
+    fwd.synchronize()
+    for it in range(nt, 0, -1):
+        # self-adjoint steps: TimeStep (Iso, TTI), TimeStepLinear (VTI), as propagateadjoint does
+        adj.step_async(1, linear=shot["physics"] == "vti")
+        pc = ct.c_void_p(ct.cast(adj.abi.getPCur(adj.p), ct.c_void_p).value)
+        _lib.check(lib.WFD_Inject(tadj, pc, ct.c_void_p(data.data_ptr()), it, shot["nt"], ct.c_void_p(adj.stream())),
+                   "inject adjoint")
+        if it % every == 0:
+            k = it // every - 1
+            f = store.get(k, as_)
+            wf = {"pspace": f[0]}
+            if aniso:
+                wf["mspace"] = f[1]
+            props.adjointBornAccumulation(adj, mtype, ic, {"v": image}, wf)
+            if hasattr(store, "release"):
+                store.release(k, as_)
+    adj.synchronize()
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    lib.WFD_Points_Free(tsrc)
+    lib.WFD_Points_Free(tadj)
+    props.free(fwd)
+    props.free(adj)
+    return image, secs
