@@ -35,6 +35,20 @@ def _field(prop, name, shape):
     return torch.as_tensor(_CAI(ptr, shape), device="cuda")
 
 
+class _PCur:
+    """pCur of an object across its pointer swaps, without a getter call per step (a getter marks the
+    object's managed arrays as touched by the host, which makes the next drop-in call move them)."""
+
+    def __init__(self, prop):
+        self.a = ct.cast(prop.abi.getPCur(prop.p), ct.c_void_p).value
+        self.b = ct.cast(prop.abi.getPOld(prop.p), ct.c_void_p).value
+        self.n = 0
+
+    def step(self):
+        self.n += 1
+        return ct.c_void_p(self.b if self.n & 1 else self.a)
+
+
 class DeviceStore:
     def __init__(self, shape, nsnap, nfields):
         import torch
@@ -187,20 +201,19 @@ def born_data(shot):
     trec = lib.WFD_Points_Create(shot["rec"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["rec"]), 1)
     data = torch.zeros(len(shot["rec"]) * nt, device="cuda")
     mtype = getattr(props, p1.NAME + "_Model_V")()
+    wf = {"pspace": _field(p0, "PSpace", shape)}
+    if shot["physics"] != "iso":
+        wf["mspace"] = _field(p0, "MSpace", shape)
+    c0, c1 = _PCur(p0), _PCur(p1)
     for it in range(1, nt + 1):
         p0.step_async(1)
-        pc = ct.c_void_p(ct.cast(p0.abi.getPCur(p0.p), ct.c_void_p).value)
-        _lib.check(lib.WFD_Inject(tsrc, pc, ct.c_void_p(shot["wavelet"].data_ptr()), it, nt,
+        _lib.check(lib.WFD_Inject(tsrc, c0.step(), ct.c_void_p(shot["wavelet"].data_ptr()), it, nt,
                                   ct.c_void_p(p0.stream())), "inject")
         p0.synchronize()
         props.scale_spatial_derivatives(p0)
-        wf = {"pspace": _field(p0, "PSpace", shape)}
-        if shot["physics"] != "iso":
-            wf["mspace"] = _field(p0, "MSpace", shape)
         props.propagateforward(p1)
         props.forwardBornInjection(p1, mtype, {"v": shot["dv"]}, wf)
-        pc1 = ct.c_void_p(ct.cast(p1.abi.getPCur(p1.p), ct.c_void_p).value)
-        _lib.check(lib.WFD_Extract(trec, ct.c_void_p(data.data_ptr()), pc1, it, nt, ct.c_void_p(p1.stream())),
+        _lib.check(lib.WFD_Extract(trec, ct.c_void_p(data.data_ptr()), c1.step(), it, nt, ct.c_void_p(p1.stream())),
                    "extract")
         p1.synchronize()
     lib.WFD_Points_Free(tsrc)
@@ -229,24 +242,24 @@ def born_image(shot, data, store, every=4, nt=None):
     ic = props.ImagingConditionStandard()
     fs = torch.cuda.ExternalStream(fwd.stream())
     as_ = torch.cuda.ExternalStream(adj.stream())
+    f_space = [_field(fwd, "PSpace", shape)] + ([_field(fwd, "MSpace", shape)] if aniso else [])
+    fcur, acur = _PCur(fwd), _PCur(adj)
+    props.scale_spatial_derivatives(adj)  # the device call after the getters (moves the arrays once)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for it in range(1, nt + 1):
         fwd.step_async(1)
-        pc = ct.c_void_p(ct.cast(fwd.abi.getPCur(fwd.p), ct.c_void_p).value)
-        _lib.check(lib.WFD_Inject(tsrc, pc, ct.c_void_p(shot["wavelet"].data_ptr()), it, shot["nt"],
+        _lib.check(lib.WFD_Inject(tsrc, fcur.step(), ct.c_void_p(shot["wavelet"].data_ptr()), it, shot["nt"],
                                   ct.c_void_p(fwd.stream())), "inject")
         if it % every == 0:
             props.scale_spatial_derivatives(fwd)
-            f = [_field(fwd, "PSpace", shape)] + ([_field(fwd, "MSpace", shape)] if aniso else [])
-            store.put(it // every - 1, f, fs)
+            store.put(it // every - 1, f_space, fs)
     fwd.synchronize()
     for it in range(nt, 0, -1):
         # self-adjoint steps: TimeStep (Iso, TTI), TimeStepLinear (VTI), as propagateadjoint does
         adj.step_async(1, linear=shot["physics"] == "vti")
-        pc = ct.c_void_p(ct.cast(adj.abi.getPCur(adj.p), ct.c_void_p).value)
-        _lib.check(lib.WFD_Inject(tadj, pc, ct.c_void_p(data.data_ptr()), it, shot["nt"], ct.c_void_p(adj.stream())),
-                   "inject adjoint")
+        _lib.check(lib.WFD_Inject(tadj, acur.step(), ct.c_void_p(data.data_ptr()), it, shot["nt"],
+                                  ct.c_void_p(adj.stream())), "inject adjoint")
         if it % every == 0:
             k = it // every - 1
             f = store.get(k, as_)
