@@ -47,6 +47,10 @@ WORKLOADS = {
                    nt=2000, nsponge=40, fpeak=12.0, nrec=(256, 256), bytes_per_cell=56,
                    label="3D AcoVTIDenQ forward, 400^3 (64M cells), 10 m, dt 0.5 ms, nt 2000, 40-cell sponge, "
                          "12 Hz Ricker, 256x256 surface receivers"),
+    # profiling-size case of the VTI kernel (fields still larger than L2: 67 MB each)
+    "vti256": dict(physics="vti", name="Prop3DAcoVTIDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
+                   nt=2000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=56,
+                   label="3D AcoVTIDenQ forward, 256^3 (16.8M cells), profiling size"),
     # profiling-size case of the TTI kernel (fields still larger than L2: 67 MB each)
     "tti256": dict(physics="tti", name="Prop3DAcoTTIDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
                    nt=2000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=72,

@@ -11,11 +11,18 @@ bool fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream
         if (fused_iso3d_tma(g, F, s)) return true;
         return fused_iso3d(g, F, s);
     }
-    if (g.ndim == 3 && (phys == VTI || phys == TTI)) return fused_aniso3d_tma(g, phys, linear, F, s);
+    if (g.ndim == 3 && phys == VTI) {
+        // the VTI kernel with x-direction register queues, else the ring-staged kernel TTI uses
+        if (fused_vti3d_tma(g, linear, F, s)) return true;
+        return fused_aniso3d_tma(g, phys, linear, F, s);
+    }
+    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, F, s);
     return false;
 }
 
 // timeout flags of every fused kernel, cleared on read
-unsigned fused_status_and_clear() { return iso3d_status_and_clear() | aniso3d_status_and_clear(); }
+unsigned fused_status_and_clear() {
+    return iso3d_status_and_clear() | aniso3d_status_and_clear() | vti3d_status_and_clear();
+}
 
 }  // namespace WFD_NS

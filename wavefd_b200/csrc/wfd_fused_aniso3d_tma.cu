@@ -609,7 +609,8 @@ bool fused_aniso3d_tma(const Grid &g, int phys, int linear, const Fields &F, cud
 }
 
 bool aniso3d_tma_describe(const Grid &g, int phys, const Fields &F, int xchunk, AnisoShotDesc *d, TileInfo *t) {
-    if (g.ndim != 3 || g.nz % 4 != 0 || xchunk < 1 || (phys != VTI && phys != TTI)) return false;
+    if (phys == VTI) return vti3d_tma_describe(g, F, xchunk, d, t);  // batched VTI uses the queue kernel
+    if (g.ndim != 3 || g.nz % 4 != 0 || xchunk < 1 || phys != TTI) return false;
     if (d) {
         if (!aniso_maps(g, phys, F, d->m)) return false;
         d->pold = F.pold;
@@ -627,7 +628,7 @@ bool aniso3d_tma_describe(const Grid &g, int phys, const Fields &F, int xchunk, 
         t->tz = TZ;
         t->ty = TY;
         t->warmup = WARMUP;
-        t->grid_cap = phys == TTI ? aniso_grid_cap<TTI, false>() : aniso_grid_cap<VTI, false>();
+        t->grid_cap = aniso_grid_cap<TTI, false>();
     }
     return true;
 }
@@ -639,9 +640,7 @@ void aniso3d_tma_batch(const Grid &gc, int phys, const AnisoShotDesc *shots, con
         k_aniso3d_tma<TTI, false, true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, AnisoMaps{}, 0, 0, 0, 1, shots,
                                                                      sel, items, nitems, counter);
     } else {
-        aniso_grid_cap<VTI, false>();
-        k_aniso3d_tma<VTI, false, true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, AnisoMaps{}, 0, 0, 0, 1, shots,
-                                                                     sel, items, nitems, counter);
+        vti3d_tma_batch(gc, shots, sel, items, nitems, counter, grid, s);
     }
 }
 

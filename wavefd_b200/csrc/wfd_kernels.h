@@ -67,6 +67,12 @@ struct TileInfo {
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
+    bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \
+    bool vti3d_tma_describe(const wfd::Grid &g, const wfd::Fields &F, int xchunk, wfd::AnisoShotDesc *d, \
+                            wfd::TileInfo *t);                                                           \
+    void vti3d_tma_batch(const wfd::Grid &gc, const wfd::AnisoShotDesc *shots, const int *sel,          \
+                         const int2 *items, int nitems, int *counter, int grid, cudaStream_t s);        \
+    unsigned vti3d_status_and_clear();                                                                   \
     unsigned iso3d_status_and_clear();                                                                   \
     /* batched launches over many shots (descriptors and items in device memory) */                     \
     bool iso3d_tma_describe(const wfd::Grid &g, const wfd::Fields &F, int xchunk, wfd::IsoShotDesc *d,   \
