@@ -20,8 +20,9 @@
 // depends on the order CTAs reach them; everything else is deterministic.
 //
 // Inference (encode / decode) runs the four layers as BF16 tensor-core MMAs (mma.sync m16n8k16,
-// FP32 accumulate) on slabs of 32(z) x 32(y) x 8(x) cells staged in shared memory; at about 12
-// flop per byte it is bound by HBM, not by the tensor pipe. Training runs forward and backward on
+// FP32 accumulate) on slabs of 32(z) x 32(y) x 8(x) cells staged in shared memory (the encoder
+// double-buffers them with cp.async); at about 12 flop per byte it is bound by HBM, not by the
+// tensor pipe. Training runs forward and backward on
 // CUDA cores in FP32 from the same BF16 weights and BF16-rounded activations (straight-through
 // gradients of the roundings), then Adam on FP32 master weights.
 //
@@ -95,6 +96,12 @@ __device__ __forceinline__ long block_id(const Dims &d, int xi, int yi, int zi, 
     return ((long)bx * d.nby + by) * d.nbz + bz;
 }
 
+// Slab layout in shared memory: row (x, y) holds 32 z values, z stored at z ^ swz(x, y). The XOR
+// touches bits 2-4 only (float4 groups stay whole) and spreads the rows of a fragment load over
+// the banks (the sub-blocks of a fragment differ in x bit 2, y bit 2 and y bit 0).
+__device__ __forceinline__ int swz(int x, int y) { return (((x >> 2) & 1) << 4) | (((y >> 2) & 1) << 3) | ((y & 1) << 2); }
+__device__ __forceinline__ int soff(int x, int y, int z) { return (x * SY + y) * SZ + (z ^ swz(x, y)); }
+
 // slab load (zero outside the grid) into sm[x][y][z]
 __device__ __forceinline__ void load_slab(const Dims &d, const float *__restrict__ f, int xi, int yi, int zi,
                                           float *sm) {
@@ -115,8 +122,25 @@ __device__ __forceinline__ void load_slab(const Dims &d, const float *__restrict
                 v.w = gz + 3 < d.nz ? p[3] : 0.f;
             }
         }
-        *reinterpret_cast<float4 *>(sm + (x * SY + y) * SZ + z) = v;
+        *reinterpret_cast<float4 *>(sm + soff(x, y, z)) = v;
     }
+}
+
+// the same load with cp.async (16-byte copies, zero fill outside the grid); needs nz % 4 == 0 and a
+// 16-byte-aligned field. Completion: cp.async.wait_group, then a CTA barrier.
+__device__ __forceinline__ void load_slab_async(const Dims &d, const float *__restrict__ f, int xi, int yi, int zi,
+                                                float *sm) {
+    const int x0 = xi * SX, y0 = yi * SY, z0 = zi * SZ;
+    for (int q = threadIdx.x; q < SLAB / 4; q += NTC) {
+        const int z = (q % (SZ / 4)) * 4, y = (q / (SZ / 4)) % SY, x = q / (SZ / 4 * SY);
+        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
+        const bool in = gx < d.nx && gy < d.ny && gz < d.nz;
+        const float *src = in ? f + ((long)gx * d.ny + gy) * d.nz + gz : f;
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(sm + soff(x, y, z)));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 __device__ __forceinline__ void store_slab(const Dims &d, float *__restrict__ f, int xi, int yi, int zi,
@@ -127,7 +151,7 @@ __device__ __forceinline__ void store_slab(const Dims &d, float *__restrict__ f,
         const int z = (q % (SZ / 4)) * 4, y = (q / (SZ / 4)) % SY, x = q / (SZ / 4 * SY);
         const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
         if (gx >= d.nx || gy >= d.ny || gz >= d.nz) continue;
-        const float4 v = *reinterpret_cast<const float4 *>(sm + (x * SY + y) * SZ + z);
+        const float4 v = *reinterpret_cast<const float4 *>(sm + soff(x, y, z));
         float *p = f + ((long)gx * d.ny + gy) * d.nz + gz;
         if (vec && gz + 3 < d.nz) {
             *reinterpret_cast<float4 *>(p) = v;
@@ -146,18 +170,18 @@ __device__ __forceinline__ int cell_off(int r, int k) {
     const int x = (s >> 2) * 4 + (k >> 4);
     const int y = (b >> 2) * 8 + ((s >> 1) & 1) * 4 + ((k >> 2) & 3);
     const int z = (b & 3) * 8 + (s & 1) * 4 + (k & 3);
-    return (x * SY + y) * SZ + z;
+    return soff(x, y, z);
 }
 
 // ---- encode -----------------------------------------------------------------------------------------
 // Codes and scales of every block, and its error energy: the block is decoded here too (D1, D2 on
 // the same tiles) and sum((decoded - field)^2) over its cells is stored in err_out.
-__global__ void __launch_bounds__(NTC, 3)
+__global__ void __launch_bounds__(NTC, 2)
     k_encode(Dims d, const float *__restrict__ f, const bf16 *__restrict__ wb, const float *__restrict__ wp,
              float *__restrict__ scale_out, float *__restrict__ err_out, bf16 *__restrict__ lat_out) {
     extern __shared__ __align__(16) float smf[];
-    float *slab = smf;                                     // SLAB floats
-    float *bscale = slab + SLAB;                           // 16
+    float *slabs = smf;                                    // 2 x SLAB floats (double buffer)
+    float *bscale = slabs + 2 * SLAB;                      // 16
     float *binv = bscale + 16;                             // 16
     float *berr = binv + 16;                               // 16
     float *sb1 = berr + 16;                                // 16
@@ -180,20 +204,40 @@ __global__ void __launch_bounds__(NTC, 3)
     sb3[tid] = wp[OFF_B3 + tid];
     if (tid < 64) sb4[tid] = wp[OFF_B4 + tid];
     const long nslab = (long)d.nsx * d.nsy * d.nsz;
-    for (long sl = blockIdx.x; sl < nslab; sl += gridDim.x) {
+    const bool async = (d.nz % 4) == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0;
+    if (async && blockIdx.x < nslab) {
+        int xi, yi, zi;
+        slab_of(d, blockIdx.x, xi, yi, zi);
+        load_slab_async(d, f, xi, yi, zi, slabs);
+    }
+    int buf = 0;
+    for (long sl = blockIdx.x; sl < nslab; sl += gridDim.x, buf ^= 1) {
         int xi, yi, zi;
         slab_of(d, sl, xi, yi, zi);
-        __syncthreads();  // previous slab's readers are done
-        load_slab(d, f, xi, yi, zi, slab);
+        float *slab = slabs + buf * SLAB;
+        __syncthreads();  // the other buffer's readers (the previous slab) are done
+        if (async) {
+            // the next slab's copies go into the other buffer while this one is processed
+            if (sl + gridDim.x < nslab) {
+                int xn, yn, zn;
+                slab_of(d, sl + gridDim.x, xn, yn, zn);
+                load_slab_async(d, f, xn, yn, zn, slabs + (buf ^ 1) * SLAB);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+        } else {
+            load_slab(d, f, xi, yi, zi, slab);
+        }
         __syncthreads();
         {  // block max |value|: 8 threads per block, one x plane each
             const int b = tid >> 3, x = tid & 7;
-            const float *p = slab + (x * SY + (b >> 2) * 8) * SZ + (b & 3) * 8;
             float m = 0.0f;
 #pragma unroll
-            for (int y = 0; y < 8; y++) {
-                const float4 u = *reinterpret_cast<const float4 *>(p + y * SZ);
-                const float4 v = *reinterpret_cast<const float4 *>(p + y * SZ + 4);
+            for (int yy = 0; yy < 8; yy++) {
+                const int y = (b >> 2) * 8 + yy, z = (b & 3) * 8;
+                const float4 u = *reinterpret_cast<const float4 *>(slab + soff(x, y, z));
+                const float4 v = *reinterpret_cast<const float4 *>(slab + soff(x, y, z + 4));
                 m = fmaxf(m, fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w))));
                 m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
             }
@@ -467,7 +511,7 @@ __global__ void __launch_bounds__(NTC, 4)
     }
 }
 
-constexpr size_t ENC_SMEM = (size_t)(SLAB + 16 * 4 + 32 + 128 + 64) * 4 +
+constexpr size_t ENC_SMEM = (size_t)(2 * SLAB + 16 * 4 + 32 + 128 + 64) * 4 +
                             (size_t)(16 * HROW + 16 * LATP + 16 * W1P + 32 * W2P + 128 * W3P + 64 * W4P) * 2;
 constexpr size_t DEC_SMEM =
     (size_t)(SLAB + 16 + 128 + 64) * 4 + (size_t)(16 * LATP + 16 * HROW + 128 * W3P + 64 * W4P) * 2;
