@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
           "--expt-relaxed-constexpr"]
 STRICT = ["-DWFD_STRICT=1", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-FAST = ["-DWFD_STRICT=0", "-fmad=true", "-prec-div=false", "-prec-sqrt=true", "-ftz=true"]
+FAST = ["-DWFD_STRICT=0", "-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 
 KERNEL_SOURCES = ["wfd_generic.cu", "wfd_fused.cu", "wfd_fused_iso3d.cu", "wfd_fused_iso3d_tma.cu",
                   "wfd_fused_aniso3d_tma.cu", "wfd_fused_vti3d_tma.cu", "wfd_wavefieldsep.cu"]
