@@ -248,6 +248,21 @@ void extractdata_float(float *data, float *field, SourcePoint32 **partitions, si
 void extractdata_double(double *data, double *field, SourcePoint64 **partitions, size_t npartitions,
                         long *npoints_per_partition, size_t it, size_t nt, size_t nthreads);
 
+/* ---- src/spacetime.cc:228-330: time interpolation dtmod <-> dtrec (filters from interpfilters,
+ * src/spacetime.jl:333-360; nh pointers to 8 taps each; traces contiguous in time; nd >= 7) ---- */
+void interpadjoint_1d_float(float **h, float *m, float *d, size_t nh, size_t nm, size_t nd);
+void interpadjoint_1d_double(double **h, double *m, double *d, size_t nh, size_t nm, size_t nd);
+void interpforward_1d_float(float **h, float *d, float *m, size_t nh, size_t nd, size_t nm);
+void interpforward_1d_double(double **h, double *d, double *m, size_t nh, size_t nd, size_t nm);
+void interpadjoint_nd_float(float **h, float *m, float *d, size_t nh, size_t nm, size_t nd, size_t nslow,
+                            size_t nthreads);
+void interpadjoint_nd_double(double **h, double *m, double *d, size_t nh, size_t nm, size_t nd, size_t nslow,
+                             size_t nthreads);
+void interpforward_nd_float(float **h, float *d, float *m, size_t nh, size_t nd, size_t nm, size_t nslow,
+                            size_t nthreads);
+void interpforward_nd_double(double **h, double *d, double *m, size_t nh, size_t nd, size_t nm, size_t nslow,
+                             size_t nthreads);
+
 /* ======================================================================================== */
 /* Part 2: add-on entry points (no counterpart in the reference)                            */
 /* ======================================================================================== */
@@ -288,6 +303,19 @@ long WFD_Points_Groups(void *table);
 int WFD_Inject(void *table, float *field, const float *data, long it, long nt, void *stream);
 /* data[(ir-1)*nt + it-1] += c * field[iu-1] on the device */
 int WFD_Extract(void *table, float *data, const float *field, long it, long nt, void *stream);
+
+/* Time interpolation on device arrays (the arithmetic of interpforward_nd_float (forward != 0:
+ * out = nd x nslow coarse from in = nm x nslow fine) or interpadjoint_nd_float), h = nh x 8 taps
+ * in device memory, asynchronous on `stream`. */
+int WFD_Interp(int forward, const float *h, float *out, const float *in, long nh, long nm, long nd, long nslow,
+               void *stream);
+/* Receiver extraction streamed into the forward time interpolation: at fine step it (1-based, of
+ * nm) each receiver trace's sample (field values through a WFD_Points_Create(..., 1) table) is
+ * added into the coarse traces (nd x ntraces, zeroed by the caller before the first step) with
+ * the taps h (device, nh x 8); after the last step the coarse traces equal extractdata into a fine
+ * buffer followed by interpforward_nd_float, bit for bit, with no fine buffer. */
+int WFD_ExtractInterp(void *table, float *coarse, const float *field, const float *h, long nh, long it, long nm,
+                      long nd, void *stream);
 
 /* Batched shots (no counterpart in the reference, whose Ginsu is exported but not defined,
  * src/WaveFD.jl:52). A batch advances many 3D objects made by the *_alloc calls above (uneven sizes;

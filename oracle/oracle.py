@@ -118,6 +118,14 @@ class Oracle:
         self.lib.wfo_inject(_p(field), _p(data_colmajor), c_long(it), c_long(nt), iu.ctypes.data_as(_i64p),
                             ir.ctypes.data_as(_i64p), _p(c), c_long(len(c)))
 
+    def interp(self, forward, h, out, inp, nh, nout, nin, nslow):
+        """Time interpolation (wfo_interpforward_* / wfo_interpadjoint_*), float32 or float64 arrays."""
+        dbl = out.dtype == np.float64
+        ptr = (lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) if dbl else _p
+        name = ("wfo_interpforward_" if forward else "wfo_interpadjoint_") + ("double" if dbl else "float")
+        getattr(self.lib, name)(ptr(np.ascontiguousarray(h)), ptr(out), ptr(inp), c_long(nh), c_long(nout),
+                                c_long(nin), c_long(nslow))
+
     def extract(self, data_colmajor, field, it, nt, iu, ir, c):
         iu = np.ascontiguousarray(iu, dtype=np.int64)
         ir = np.ascontiguousarray(ir, dtype=np.int64)

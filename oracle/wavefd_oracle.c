@@ -831,3 +831,59 @@ void wfo_extract(float *data, const float *field, long it, long nt, const long *
                  const float *c, long n) {
     for (long i = 0; i < n; i++) data[(ir[i] - 1) * nt + it - 1] += c[i] * field[iu[i] - 1];
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* Time interpolation between dtmod (fine, nm samples) and dtrec (coarse, nd samples) with nh
+ * 8-tap filters h[k][0..7]; traces are contiguous in time, nslow traces. spacetime.cc:4-127:
+ * the coarse index i runs over the helper calls (i, lo, hi) = (0,3,7), (1,2,7), (2,1,7),
+ * (3..nd-5, 0,7), (nd-4,0,6), (nd-3,0,5), (nd-2,0,4); fine sample jk = i*nh + k (if < nm) pairs
+ * with coarse samples i-3+l, l in [lo, hi]. Adjoint: m[jk] += h[k][l] d[i-3+l] (m zeroed first);
+ * forward: d[i-3+l] += h[k][l] m[jk] (d zeroed first), in that loop order. Needs nd >= 7. */
+#define WFO_INTERP(T, SUF)                                                                           \
+    static void wfo_interp_calls_##SUF(long nd, long *ci, long *clo, long *chi, long *ncalls) {     \
+        long n = 0;                                                                                  \
+        ci[n] = 0, clo[n] = 3, chi[n++] = 7;                                                         \
+        ci[n] = 1, clo[n] = 2, chi[n++] = 7;                                                         \
+        ci[n] = 2, clo[n] = 1, chi[n++] = 7;                                                         \
+        for (long i = 3; i < nd - 4; i++) ci[n] = i, clo[n] = 0, chi[n++] = 7;                       \
+        ci[n] = nd - 4, clo[n] = 0, chi[n++] = 6;                                                    \
+        ci[n] = nd - 3, clo[n] = 0, chi[n++] = 5;                                                    \
+        ci[n] = nd - 2, clo[n] = 0, chi[n++] = 4;                                                    \
+        *ncalls = n;                                                                                 \
+    }                                                                                                \
+    void wfo_interpadjoint_##SUF(const T *h, T *m, const T *d, long nh, long nm, long nd, long nslow) { \
+        long *ci = malloc(sizeof(long) * (nd + 8)), *clo = malloc(sizeof(long) * (nd + 8)),         \
+             *chi = malloc(sizeof(long) * (nd + 8)), nc;                                              \
+        wfo_interp_calls_##SUF(nd, ci, clo, chi, &nc);                                               \
+        for (long t = 0; t < nslow; t++) {                                                           \
+            T *mt = m + t * nm;                                                                      \
+            const T *dt = d + t * nd;                                                                \
+            for (long j = 0; j < nm; j++) mt[j] = 0;                                                 \
+            for (long c = 0; c < nc; c++)                                                            \
+                for (long k = 0; k < nh; k++) {                                                      \
+                    const long jk = ci[c] * nh + k;                                                  \
+                    if (jk >= nm) continue;                                                          \
+                    for (long l = clo[c]; l <= chi[c]; l++) mt[jk] += h[k * 8 + l] * dt[ci[c] - 3 + l]; \
+                }                                                                                    \
+        }                                                                                            \
+        free(ci), free(clo), free(chi);                                                              \
+    }                                                                                                \
+    void wfo_interpforward_##SUF(const T *h, T *d, const T *m, long nh, long nd, long nm, long nslow) { \
+        long *ci = malloc(sizeof(long) * (nd + 8)), *clo = malloc(sizeof(long) * (nd + 8)),         \
+             *chi = malloc(sizeof(long) * (nd + 8)), nc;                                              \
+        wfo_interp_calls_##SUF(nd, ci, clo, chi, &nc);                                               \
+        for (long t = 0; t < nslow; t++) {                                                           \
+            T *dt = d + t * nd;                                                                      \
+            const T *mt = m + t * nm;                                                                \
+            for (long i = 0; i < nd; i++) dt[i] = 0;                                                 \
+            for (long c = 0; c < nc; c++)                                                            \
+                for (long k = 0; k < nh; k++) {                                                      \
+                    const long jk = ci[c] * nh + k;                                                  \
+                    if (jk >= nm) continue;                                                          \
+                    for (long l = clo[c]; l <= chi[c]; l++) dt[ci[c] - 3 + l] += h[k * 8 + l] * mt[jk]; \
+                }                                                                                    \
+        }                                                                                            \
+        free(ci), free(clo), free(chi);                                                              \
+    }
+WFO_INTERP(float, float)
+WFO_INTERP(double, double)

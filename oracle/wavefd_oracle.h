@@ -75,6 +75,12 @@ void wfo_inject(float *field, const float *data, long it, long nt, const long *i
 void wfo_extract(float *data, const float *field, long it, long nt, const long *iu, const long *ir,
                  const float *c, long n);
 
+/* spacetime.cc:4-127 time interpolation (h: nh x 8 filters, row-major), nslow traces; nd >= 7 */
+void wfo_interpadjoint_float(const float *h, float *m, const float *d, long nh, long nm, long nd, long nslow);
+void wfo_interpforward_float(const float *h, float *d, const float *m, long nh, long nd, long nm, long nslow);
+void wfo_interpadjoint_double(const double *h, double *m, const double *d, long nh, long nm, long nd, long nslow);
+void wfo_interpforward_double(const double *h, double *d, const double *m, long nh, long nd, long nm, long nslow);
+
 #ifdef __cplusplus
 }
 #endif

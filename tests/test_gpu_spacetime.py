@@ -112,3 +112,74 @@ def test_device_tables_inject_extract(lib, oracle):
     assert same(dd.cpu().numpy(), d_or)
     lib.WFD_Points_Free(tin)
     lib.WFD_Points_Free(tout)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nh,nd", [(1, 7), (4, 13), (8, 250)])
+def test_time_interpolation_dropin_bitwise(lib, oracle, dtype, nh, nd):
+    """interp{forward,adjoint}_nd_{float,double} (spacetime.cc:228-330) on the GPU, host arrays, against
+    the restatement (pinned to the compiled reference)."""
+    from wavefd_b200.spacetime import interp, interpfilters
+    st = SpacetimeABI(lib)
+    rng = np.random.default_rng(nh + nd)
+    h = interpfilters(0.0005, 0.0005 * nh, dtype=dtype)
+    nm = nd * nh - nh // 2
+    fine = rng.standard_normal((5, nm)).astype(dtype)
+    coarse = rng.standard_normal((5, nd)).astype(dtype)
+    got_f = interp(st, True, h, fine, nd)
+    got_a = interp(st, False, h, coarse, nm)
+    want_f, want_a = np.zeros_like(got_f), np.zeros_like(got_a)
+    oracle.interp(True, h, want_f, fine, nh, nd, nm, 5)
+    oracle.interp(False, h, want_a, coarse, nh, nm, nd, 5)
+    assert np.array_equal(got_f, want_f)
+    assert np.array_equal(got_a, want_a)
+
+
+def test_time_interpolation_device_and_streamed_extraction(lib, oracle):
+    """WFD_Interp on device arrays, and WFD_ExtractInterp (extraction streamed into the forward
+    interpolation) against extraction into a fine buffer followed by interpforward: bitwise."""
+    import torch
+    from wavefd_b200.spacetime import interpfilters
+    nh, nd = 4, 60
+    nm = nd * nh
+    h = interpfilters(0.0005, 0.002)
+    dh = torch.from_numpy(h).cuda()
+    rng = np.random.default_rng(3)
+    # device interpolation, both directions
+    fine = rng.standard_normal((7, nm)).astype(np.float32)
+    coarse = rng.standard_normal((7, nd)).astype(np.float32)
+    out_f = torch.zeros((7, nd), device="cuda")
+    out_a = torch.zeros((7, nm), device="cuda")
+    assert lib.WFD_Interp(1, ctypes.c_void_p(dh.data_ptr()), ctypes.c_void_p(out_f.data_ptr()),
+                          ctypes.c_void_p(torch.from_numpy(fine).cuda().data_ptr()), nh, nm, nd, 7, None) == 0
+    assert lib.WFD_Interp(0, ctypes.c_void_p(dh.data_ptr()), ctypes.c_void_p(out_a.data_ptr()),
+                          ctypes.c_void_p(torch.from_numpy(coarse).cuda().data_ptr()), nh, nm, nd, 7, None) == 0
+    torch.cuda.synchronize()
+    want_f, want_a = np.zeros((7, nd), np.float32), np.zeros((7, nm), np.float32)
+    oracle.interp(True, h, want_f, fine, nh, nd, nm, 7)
+    oracle.interp(False, h, want_a, coarse, nh, nm, nd, 7)
+    assert np.array_equal(out_f.cpu().numpy(), want_f)
+    assert np.array_equal(out_a.cpu().numpy(), want_a)
+    # streamed extraction: 9 receivers (one spread over 3 points) on a 2000-cell field over nm steps
+    ngrid, nrec = 2000, 9
+    iu = np.concatenate([rng.integers(1, ngrid + 1, nrec), rng.integers(1, ngrid + 1, 2)])
+    ir = np.concatenate([np.arange(1, nrec + 1), [4, 4]])
+    c = rng.standard_normal(len(iu)).astype(np.float32)
+    order = np.argsort(ir, kind="stable")
+    iu, ir, c = iu[order], ir[order], c[order]
+    pts = (SourcePoint32 * len(c))(*[SourcePoint32(int(a), int(b), float(w)) for a, b, w in zip(iu, ir, c)])
+    tab = lib.WFD_Points_Create(ctypes.cast(pts, ctypes.POINTER(SourcePoint32)), len(c), 1)
+    dcoarse = torch.zeros((nrec, nd), device="cuda")
+    fine_traces = np.zeros((nrec, nm), np.float32)
+    for it in range(1, nm + 1):
+        field = rng.standard_normal(ngrid).astype(np.float32)
+        dfield = torch.from_numpy(field).cuda()
+        assert lib.WFD_ExtractInterp(tab, ctypes.c_void_p(dcoarse.data_ptr()), ctypes.c_void_p(dfield.data_ptr()),
+                                     ctypes.c_void_p(dh.data_ptr()), nh, it, nm, nd, None) == 0
+        oracle.extract(fine_traces.reshape(-1), field, it, nm, iu, ir, c)
+        torch.cuda.synchronize()
+    lib.WFD_Points_Free(tab)
+    want = np.zeros((nrec, nd), np.float32)
+    oracle.interp(True, h, want, fine_traces, nh, nd, nm, nrec)
+    got = dcoarse.cpu().numpy()
+    assert np.array_equal(got, want), mismatch_report(got, want)

@@ -213,3 +213,27 @@ def test_inject_extract_bitwise(oracle):
     st.extractdata_float(fptr(d_ref), fptr(field), parts, 1, npp, 9, nt, 1)
     oracle.extract(d_or, field, 9, nt, iu, ir, c)
     assert same(d_ref, d_or), mismatch_report(d_ref, d_or)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nh,nd", [(1, 7), (2, 8), (4, 13), (5, 40)])
+def test_time_interpolation_bitwise(oracle, dtype, nh, nd):
+    """spacetime.cc:4-127 (interp{forward,adjoint}_nd) against the restatement, both directions."""
+    from wavefd_b200.abi import SpacetimeABI
+    from wavefd_b200.spacetime import interp, interpfilters
+    st = SpacetimeABI(reference_lib("spacetime", "strict"))
+    rng = np.random.default_rng(nh * 100 + nd)
+    h = interpfilters(0.001, 0.001 * nh, mode=0, dtype=dtype) + rng.standard_normal((nh, 8)).astype(dtype) * 1e-3
+    for nm in (nd * nh - nh + 1, nd * nh, nd * nh - 2 * nh):
+        if nm < 1:
+            continue
+        fine = rng.standard_normal((3, nm)).astype(dtype)
+        coarse = rng.standard_normal((3, nd)).astype(dtype)
+        want_f = interp(st, True, h, fine, nd)
+        want_a = interp(st, False, h, coarse, nm)
+        got_f = np.zeros_like(want_f)
+        got_a = np.zeros_like(want_a)
+        oracle.interp(True, h, got_f, fine, nh, nd, nm, 3)
+        oracle.interp(False, h, got_a, coarse, nh, nm, nd, 3)
+        assert np.array_equal(got_f, want_f), (nh, nd, nm)
+        assert np.array_equal(got_a, want_a), (nh, nd, nm)

@@ -108,10 +108,23 @@ class SourcePoint32(ctypes.Structure):
 
 
 class SpacetimeABI:
-    """spacetime.cc:144-162 (injectdata_float) and :184-204 (extractdata_float)."""
+    """spacetime.cc:144-162 (injectdata_float), :184-204 (extractdata_float) and the time
+    interpolation exports :228-330 (interp{forward,adjoint}_{1d,nd}_{float,double})."""
 
     def __init__(self, lib: ctypes.CDLL):
         self.lib = lib
+        for T, ct in (("float", c_float), ("double", ctypes.c_double)):
+            pp = POINTER(POINTER(ct))
+            p = POINTER(ct)
+            for fn, args in ((f"interpadjoint_1d_{T}", [pp, p, p, c_size_t, c_size_t, c_size_t]),
+                             (f"interpforward_1d_{T}", [pp, p, p, c_size_t, c_size_t, c_size_t]),
+                             (f"interpadjoint_nd_{T}", [pp, p, p, c_size_t, c_size_t, c_size_t, c_size_t, c_size_t]),
+                             (f"interpforward_nd_{T}", [pp, p, p, c_size_t, c_size_t, c_size_t, c_size_t, c_size_t])):
+                if hasattr(lib, fn):
+                    f = getattr(lib, fn)
+                    f.restype = None
+                    f.argtypes = args
+                    setattr(self, fn, f)
         self.injectdata_float = lib.injectdata_float
         self.injectdata_float.restype = None
         self.injectdata_float.argtypes = [_f32p, _f32p, c_size_t, c_size_t, POINTER(POINTER(SourcePoint32)),

@@ -7,6 +7,8 @@
 // location keeps that order; one thread per group then accumulates it in order.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -56,5 +58,11 @@ void build(Table<T> &t, const std::vector<PointsT<T>> &pts, int by_receiver) {
     t.start.push_back((long)order.size());
     t.ngroups = (long)t.key.size();
 }
+
+// streaming receiver extraction + forward time interpolation (wfd_interp.cu): one thread per
+// receiver group at fine sample jk
+void launch_extract_interp(long ngroups, const long *key, const long *start, const long *other, const float *c,
+                           const float *field, const float *h, long nh, long jk, long nm, long nd, float *coarse,
+                           cudaStream_t s);
 
 }  // namespace wfd

@@ -254,3 +254,13 @@ extern "C" int WFD_Extract(void *table, float *data, const float *field, long it
         d->t.ngroups, d->t.d_key, d->t.d_start, d->t.d_other, d->t.d_c, data, nt, it - 1, 0, field, 1, 0, 0);
     return cudaGetLastError() == cudaSuccess ? WFD_OK : WFD_ERR_CUDA;
 }
+
+extern "C" int WFD_ExtractInterp(void *table, float *coarse, const float *field, const float *h, long nh, long it,
+                                 long nm, long nd, void *stream) {
+    DeviceTable *d = reinterpret_cast<DeviceTable *>(table);
+    if (!d || !d->t.by_receiver || !coarse || !field || !h || nh < 1 || nd < 7 || it < 1 || it > nm) return WFD_ERR_ARG;
+    if (!d->t.ngroups) return WFD_OK;
+    wfd::launch_extract_interp(d->t.ngroups, d->t.d_key, d->t.d_start, d->t.d_other, d->t.d_c, field, h, nh, it - 1,
+                               nm, nd, coarse, (cudaStream_t)stream);
+    return cudaGetLastError() == cudaSuccess ? WFD_OK : WFD_ERR_CUDA;
+}

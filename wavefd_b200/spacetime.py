@@ -235,3 +235,39 @@ def causal_ricker(t, f=15.0, a=1.0, tol=1e-4):
     out = np.zeros_like(wav)
     out[: len(wav) - idx] = wav[idx:]
     return out
+
+
+def interpfilters(dtmod, dtrec, mode=0, dtype=np.float32):
+    """src/spacetime.jl:333-360: nh = dtrec/dtmod 8-tap sinc filters (nh x 8) mapping dtmod <-> dtrec;
+    mode 0 preserves amplitude in the forward operator (fine -> coarse), mode 1 in the adjoint. The
+    8x8 solve runs in float64 and is rounded to `dtype` (Julia solves in the element type, so the
+    taps agree to rounding; the interpolation kernels consume whatever taps they are given exactly)."""
+    n = int(round(dtrec / dtmod))
+    if abs(n * dtmod - dtrec) / dtrec > 1e-6:
+        raise ValueError(f"dtrec/dtmod must be an integer (n={n}, dtrec={dtrec}, dtmod={dtmod})")
+    d = dtmod / dtrec * np.arange(n)
+    fmax = 0.066 + 0.265 * np.log(8.0)
+    j = np.arange(1, 9)
+    a = np.sinc((j - 1) * fmax)
+    A = np.array([[a[abs(r - c)] for c in range(8)] for r in range(8)])
+    h = np.stack([np.linalg.solve(A, np.sinc((4 - j + d[i]) * fmax)) for i in range(n)])
+    if mode == 0:
+        h = h / n
+    return np.ascontiguousarray(h.astype(dtype))
+
+
+def interp(lib_abi, forward, h, inp, nout):
+    """Run a library's interpforward_nd / interpadjoint_nd on traces (ntraces, nin) -> (ntraces, nout)."""
+    h = np.ascontiguousarray(h)
+    T = "double" if h.dtype == np.float64 else "float"
+    ct = ctypes.c_double if T == "double" else ctypes.c_float
+    rows = (ctypes.POINTER(ct) * len(h))(*[h[k].ctypes.data_as(ctypes.POINTER(ct)) for k in range(len(h))])
+    inp = np.ascontiguousarray(inp, dtype=h.dtype)
+    ntr, nin = inp.shape
+    out = np.zeros((ntr, nout), dtype=h.dtype)
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ct))
+    if forward:
+        getattr(lib_abi, f"interpforward_nd_{T}")(rows, p(out), p(inp), len(h), nout, nin, ntr, 8)
+    else:
+        getattr(lib_abi, f"interpadjoint_nd_{T}")(rows, p(out), p(inp), len(h), nout, nin, ntr, 8)
+    return out
