@@ -263,6 +263,12 @@ void interpforward_nd_float(float **h, float *d, float *m, size_t nh, size_t nd,
 void interpforward_nd_double(double **h, double *d, double *m, size_t nh, size_t nd, size_t nm, size_t nslow,
                              size_t nthreads);
 
+/* ---- src/illumination.c:3-53 (libillumination): field = field^2; accum += field^2 ---- */
+void srcillum_helper_float(float *field_ginsu, size_t n, int nthreads);
+void srcillum_helper_double(double *field_ginsu, size_t n, int nthreads);
+void illum_accumulate_float(float *field_ginsu_accum, float *field_ginsu, size_t n, int nthreads);
+void illum_accumulate_double(double *field_ginsu_accum, double *field_ginsu, size_t n, int nthreads);
+
 /* ======================================================================================== */
 /* Part 2: add-on entry points (no counterpart in the reference)                            */
 /* ======================================================================================== */
@@ -294,6 +300,12 @@ int WFD_Prop_Prefetch(void *p);
 void *WFD_Prop_Stream(void *p);
 /* kernels the last time step launched: 1 = fused single-sweep kernel, 2 = the two passes */
 int WFD_Prop_StepKernels(void *p);
+/* nsteps time steps of the object (TimeStep, then injection into pCur at time index it, then
+ * extraction of pCur at it, it = it0, it0+1, ...; either table may be NULL), with every pair of steps
+ * replayed from one CUDA graph when use_graph != 0; indices beyond nt are skipped. Enqueued on the
+ * object's stream; returns after the graph launches are complete. */
+int WFD_Prop_Run(void *p, long nsteps, long it0, void *src_table, const float *wavelet, void *rec_table,
+                 float *traces, long nt, int use_graph);
 /* device-resident source/receiver tables built from a flat point list (grouped by written
  * location, contributions accumulated in list order, as the reference does partition-wise) */
 void *WFD_Points_Create(const SourcePoint32 *points, long npoints, int by_receiver);
@@ -316,6 +328,10 @@ int WFD_Interp(int forward, const float *h, float *out, const float *in, long nh
  * buffer followed by interpforward_nd_float, bit for bit, with no fine buffer. */
 int WFD_ExtractInterp(void *table, float *coarse, const float *field, const float *h, long nh, long it, long nm,
                       long nd, void *stream);
+
+/* Source illumination for the time loop: accum[i] += field[i]^2 on device arrays (the arithmetic of
+ * illum_accumulate_float), asynchronous on `stream`. */
+int WFD_IllumAccumulate(float *accum, const float *field, long n, void *stream);
 
 /* Batched shots (no counterpart in the reference, whose Ginsu is exported but not defined,
  * src/WaveFD.jl:52). A batch advances many 3D objects made by the *_alloc calls above (uneven sizes;

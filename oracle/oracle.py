@@ -118,6 +118,10 @@ class Oracle:
         self.lib.wfo_inject(_p(field), _p(data_colmajor), c_long(it), c_long(nt), iu.ctypes.data_as(_i64p),
                             ir.ctypes.data_as(_i64p), _p(c), c_long(len(c)))
 
+    def illum(self, accum, field):
+        """wfo_illum_float: field = field^2 (accum None) or accum += field^2, in place."""
+        self.lib.wfo_illum_float(_p(accum), _p(field), c_long(field.size))
+
     def interp(self, forward, h, out, inp, nh, nout, nin, nslow):
         """Time interpolation (wfo_interpforward_* / wfo_interpadjoint_*), float32 or float64 arrays."""
         dbl = out.dtype == np.float64

@@ -887,3 +887,11 @@ void wfo_extract(float *data, const float *field, long it, long nt, const long *
     }
 WFO_INTERP(float, float)
 WFO_INTERP(double, double)
+
+/* illumination.c:3-53: field = field^2 (accum NULL) or accum += field^2 */
+void wfo_illum_float(float *accum, float *field, long n) {
+    for (long i = 0; i < n; i++) {
+        if (accum) accum[i] += field[i] * field[i];
+        else field[i] = field[i] * field[i];
+    }
+}

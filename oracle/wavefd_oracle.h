@@ -81,6 +81,9 @@ void wfo_interpforward_float(const float *h, float *d, const float *m, long nh, 
 void wfo_interpadjoint_double(const double *h, double *m, const double *d, long nh, long nm, long nd, long nslow);
 void wfo_interpforward_double(const double *h, double *d, const double *m, long nh, long nd, long nm, long nslow);
 
+/* illumination.c:3-53 (float): field = field^2 when accum is NULL, else accum += field^2 */
+void wfo_illum_float(float *accum, float *field, long n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -183,3 +183,78 @@ def test_time_interpolation_device_and_streamed_extraction(lib, oracle):
     oracle.interp(True, h, want, fine_traces, nh, nd, nm, nrec)
     got = dcoarse.cpu().numpy()
     assert np.array_equal(got, want), mismatch_report(got, want)
+
+
+def test_illumination_bitwise(lib, oracle):
+    """srcillum_helper_float / illum_accumulate_float (illumination.c:3-53) on host and device arrays, and
+    the WFD_IllumAccumulate add-on, against the restatement."""
+    import torch
+    f32p = ctypes.POINTER(ctypes.c_float)
+    lib.srcillum_helper_float.argtypes = [f32p, ctypes.c_size_t, ctypes.c_int]
+    lib.illum_accumulate_float.argtypes = [f32p, f32p, ctypes.c_size_t, ctypes.c_int]
+    rng = np.random.default_rng(10)
+    f = rng.standard_normal(100003).astype(np.float32)
+    acc = rng.standard_normal(100003).astype(np.float32)
+    want = acc.copy()
+    oracle.illum(want, f.copy())
+    a = acc.copy()
+    lib.illum_accumulate_float(fptr(a), fptr(f.copy()), f.size, 4)  # host arrays
+    assert np.array_equal(a, want)
+    da, dfield = torch.from_numpy(acc.copy()).cuda(), torch.from_numpy(f).cuda()
+    assert lib.WFD_IllumAccumulate(ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(dfield.data_ptr()), f.size,
+                                   None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(da.cpu().numpy(), want)
+    g, gw = f.copy(), f.copy()
+    lib.srcillum_helper_float(fptr(g), f.size, 4)
+    oracle.illum(None, gw)
+    assert np.array_equal(g, gw)
+
+
+@pytest.mark.parametrize("name,shape", [("Prop2DAcoIsoDenQ_DEO2_FDTD", (44, 1, 38)),
+                                        ("Prop3DAcoTTIDenQ_DEO2_FDTD", (28, 22, 24))])
+@pytest.mark.parametrize("use_graph", [1, 0])
+def test_prop_run_matches_stepping(lib, name, shape, use_graph):
+    """WFD_Prop_Run (a pair of steps with injection and extraction replayed from a CUDA graph, the time
+    index on the device) against TimeStep + WFD_Inject + WFD_Extract per step: bitwise, pointer state
+    included, over an odd number of steps."""
+    import torch
+    from tests.harness import ABIRunner, make_model
+    from wavefd_b200.abi import PROPAGATORS
+    ndim, physics = PROPAGATORS[name][:2]
+    nz, ny, nx = shape
+    nt, nsteps = 30, 11
+    runs = []
+    for mode in ("run", "steps"):
+        g = ABIRunner(lib, name, shape, fs=True)
+        lib.WFD_Prop_SetStrict(ctypes.c_void_p(g.p), 1)
+        g.load(make_model(ndim, physics, shape, seed=4))
+        ncell = nz * ny * nx
+        src = (SourcePoint32 * 2)(SourcePoint32(ncell // 2 + 1, 1, 0.75), SourcePoint32(ncell // 2 + 3, 1, 0.25))
+        rec = (SourcePoint32 * 3)(*[SourcePoint32(3 + i * nz * 5, i + 1, 1.0) for i in range(3)])
+        ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), 2, 0)
+        tr = lib.WFD_Points_Create(ctypes.cast(rec, ctypes.POINTER(SourcePoint32)), 3, 1)
+        wav = torch.from_numpy(np.random.default_rng(1).standard_normal(nt).astype(np.float32)).cuda()
+        trc = torch.zeros(3 * nt, device="cuda")
+        torch.cuda.synchronize()
+        g.abi.TimeStep(g.p)  # one ordinary step first (an odd pointer parity)
+        stream = ctypes.c_void_p(lib.WFD_Prop_Stream(ctypes.c_void_p(g.p)))
+        if mode == "run":
+            assert lib.WFD_Prop_Run(ctypes.c_void_p(g.p), nsteps, 2, ts, ctypes.c_void_p(wav.data_ptr()), tr,
+                                    ctypes.c_void_p(trc.data_ptr()), nt, use_graph) == 0
+        else:
+            for it in range(2, 2 + nsteps):
+                assert lib.WFD_Prop_TimeStepAsync(ctypes.c_void_p(g.p), 1, 0) == 0
+                pc = ctypes.c_void_p(ctypes.cast(g.abi.getPCur(g.p), ctypes.c_void_p).value)
+                assert lib.WFD_Inject(ts, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, stream) == 0
+                assert lib.WFD_Extract(tr, ctypes.c_void_p(trc.data_ptr()), pc, it, nt, stream) == 0
+        assert lib.WFD_Prop_Synchronize(ctypes.c_void_p(g.p)) == 0
+        f = ["PCur", "POld", "PSpace"] + ([] if physics == "iso" else ["MCur", "MOld"])
+        runs.append(({k: g.arr(k).copy() for k in f}, trc.cpu().numpy()))
+        lib.WFD_Points_Free(ts)
+        lib.WFD_Points_Free(tr)
+        g.close()
+    (fa, ta), (fb, tb) = runs
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), (k, mismatch_report(fa[k], fb[k]))
+    assert np.array_equal(ta, tb)

@@ -237,3 +237,22 @@ def test_time_interpolation_bitwise(oracle, dtype, nh, nd):
         oracle.interp(False, h, got_a, coarse, nh, nm, nd, 3)
         assert np.array_equal(got_f, want_f), (nh, nd, nm)
         assert np.array_equal(got_a, want_a), (nh, nd, nm)
+
+
+def test_illumination_bitwise(oracle):
+    """illumination.c:3-53 (srcillum_helper_float, illum_accumulate_float) against the restatement."""
+    lib = reference_lib("illumination", "strict")
+    f32p = ctypes.POINTER(ctypes.c_float)
+    lib.srcillum_helper_float.argtypes = [f32p, ctypes.c_size_t, ctypes.c_int]
+    lib.illum_accumulate_float.argtypes = [f32p, f32p, ctypes.c_size_t, ctypes.c_int]
+    rng = np.random.default_rng(9)
+    f = rng.standard_normal(10001).astype(np.float32)
+    acc = rng.standard_normal(10001).astype(np.float32)
+    a1, a2 = acc.copy(), acc.copy()
+    lib.illum_accumulate_float(fptr(a1), fptr(f.copy()), f.size, 4)
+    oracle.illum(a2, f.copy())
+    assert np.array_equal(a1, a2)
+    g1, g2 = f.copy(), f.copy()
+    lib.srcillum_helper_float(fptr(g1), f.size, 4)
+    oracle.illum(None, g2)
+    assert np.array_equal(g1, g2)

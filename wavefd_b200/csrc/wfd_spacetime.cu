@@ -73,6 +73,26 @@ __global__ void k_scatter_groups(long ngroups, const long *__restrict__ key, con
     dst[d] = acc;
 }
 
+// the device-table scatter with the time index read from device memory (graph-captured time loops):
+// inject (by_receiver 0): field[key] += sum c * data[other*nt + it-1]; extract: data[key*nt + it-1]
+// += sum c * field[other]; skipped when it is outside 1..nt
+__global__ void k_scatter_groups_devit(long ngroups, const long *__restrict__ key, const long *__restrict__ start,
+                                       const long *__restrict__ other, const float *__restrict__ c, int by_receiver,
+                                       float *field, float *data, long nt, const long *__restrict__ d_it) {
+    const long gi = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long it = *d_it;
+    if (gi >= ngroups || it < 1 || it > nt) return;
+    float *dst = by_receiver ? data + key[gi] * nt + (it - 1) : field + key[gi];
+    float acc = *dst;
+    for (long j = start[gi]; j < start[gi + 1]; j++) {
+        const float v = by_receiver ? field[other[j]] : data[other[j] * nt + (it - 1)];
+        acc = add_rn(acc, mul_rn(c[j], v));
+    }
+    *dst = acc;
+}
+
+__global__ void k_tick(long *it) { *it += 1; }
+
 template <class T>
 __global__ void k_gather(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
                          T *dst) {
@@ -263,4 +283,75 @@ extern "C" int WFD_ExtractInterp(void *table, float *coarse, const float *field,
     wfd::launch_extract_interp(d->t.ngroups, d->t.d_key, d->t.d_start, d->t.d_other, d->t.d_c, field, h, nh, it - 1,
                                nm, nd, coarse, (cudaStream_t)stream);
     return cudaGetLastError() == cudaSuccess ? WFD_OK : WFD_ERR_CUDA;
+}
+
+// ---- add-on: a whole time loop in a CUDA graph ---------------------------------------------------------
+namespace {
+
+using wfd::Prop;
+
+int run_step(Prop *p, DeviceTable *src, const float *wav, DeviceTable *rec, float *trc, long nt, long *d_it) {
+    if (int rc = wfd::prop_step(p, false, false)) return rc;
+    float *pc = p->field[wfd::F_PCUR];
+    cudaStream_t s = p->stream;
+    if (src && src->t.ngroups)
+        wfd::k_scatter_groups_devit<<<wfd::nb(src->t.ngroups), 256, 0, s>>>(
+            src->t.ngroups, src->t.d_key, src->t.d_start, src->t.d_other, src->t.d_c, 0, pc, const_cast<float *>(wav),
+            nt, d_it);
+    if (rec && rec->t.ngroups)
+        wfd::k_scatter_groups_devit<<<wfd::nb(rec->t.ngroups), 256, 0, s>>>(
+            rec->t.ngroups, rec->t.d_key, rec->t.d_start, rec->t.d_other, rec->t.d_c, 1, pc, trc, nt, d_it);
+    wfd::k_tick<<<1, 1, 0, s>>>(d_it);
+    return cudaGetLastError() == cudaSuccess ? WFD_OK : wfd::prop_fail(p, WFD_ERR_CUDA, "time loop launch");
+}
+
+}  // namespace
+
+extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, const float *wavelet, void *rec_table,
+                            float *traces, long nt, int use_graph) {
+    wfd::Prop *p = reinterpret_cast<wfd::Prop *>(prop);
+    DeviceTable *src = reinterpret_cast<DeviceTable *>(src_table), *rec = reinterpret_cast<DeviceTable *>(rec_table);
+    if (!p || nsteps < 0 || (src && (src->t.by_receiver || !wavelet)) || (rec && (!rec->t.by_receiver || !traces)))
+        return WFD_ERR_ARG;
+    if (p->status) return p->status;
+    cudaStream_t s = p->stream;
+    // scratch of the unfused passes must exist before a capture (no allocation inside a graph)
+    if (!p->fused || p->ndim == 2 || p->nz % 4 != 0)
+        if (!wfd::ensure_scratch(p, p->phys == wfd::ISO ? 3 : 6)) return p->status;
+    long *d_it = nullptr;
+    if (cudaMallocAsync(&d_it, sizeof(long), s) != cudaSuccess)
+        return wfd::prop_fail(p, WFD_ERR_ALLOC, "time index allocation failed");
+    cudaMemcpyAsync(d_it, &it0, sizeof(long), cudaMemcpyHostToDevice, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
+    long done = 0;
+    int rc = WFD_OK;
+    if (use_graph && nsteps >= 2) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rc = wfd::prop_fail(p, WFD_ERR_CUDA, "begin capture");
+        } else {
+            // two steps: the pointer swap of each is done on the host during the capture, so the
+            // graph replays the pair with the pointers back where they started
+            rc = run_step(p, src, wavelet, rec, traces, nt, d_it);
+            if (!rc) rc = run_step(p, src, wavelet, rec, traces, nt, d_it);
+            const cudaError_t e = cudaStreamEndCapture(s, &graph);
+            if (!rc && e != cudaSuccess) rc = wfd::prop_fail(p, WFD_ERR_CUDA, "end capture");
+            if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+                rc = wfd::prop_fail(p, WFD_ERR_CUDA, "graph instantiation");
+            if (graph) cudaGraphDestroy(graph);
+            p->steps -= 2;  // counted again per replay
+            for (; !rc && done + 2 <= nsteps; done += 2) {
+                if (cudaGraphLaunch(exec, s) != cudaSuccess) rc = wfd::prop_fail(p, WFD_ERR_CUDA, "graph launch");
+                p->steps += 2;
+            }
+            if (exec) {
+                cudaStreamSynchronize(s);
+                cudaGraphExecDestroy(exec);
+            }
+        }
+    }
+    for (; !rc && done < nsteps; done++) rc = run_step(p, src, wavelet, rec, traces, nt, d_it);
+    cudaFreeAsync(d_it, s);
+    return rc;
 }

@@ -110,3 +110,17 @@ def center_source(shape, d, depth=2.5):
     nx, ny, nz = shape
     return hickscoeffs(d, d, 0.0, 0.0, nz, nx, [depth * d], [(nx // 2 + 0.5) * d], dy=d, y0=0.0, ny=ny,
                        y=[(ny // 2 + 0.5) * d])
+
+
+def surface_acquisition_2d(shape, d, depth=1.0):
+    """2D: a Hicks source at the centre of the top row and on-grid receivers on every surface cell
+    (depth index 2). shape = (nx, nz). Returns (sources, receivers) SourcePoint32 arrays."""
+    from .spacetime import SOURCEPOINT32, hickscoeffs
+    nx, nz = shape
+    src = hickscoeffs(d, d, 0.0, 0.0, nz, nx, [depth * d], [(nx // 2) * d])
+    iu = 3 + np.arange(nx) * nz  # 1-based (z index 2, x)
+    rec = np.zeros(nx, SOURCEPOINT32)
+    rec["iu"] = iu
+    rec["ir"] = np.arange(1, nx + 1)
+    rec["c"] = 1.0
+    return src, rec
