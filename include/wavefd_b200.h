@@ -298,8 +298,13 @@ int WFD_Prop_Synchronize(void *p);
 int WFD_Prop_Prefetch(void *p);
 /* the object's CUDA stream (a cudaStream_t) */
 void *WFD_Prop_Stream(void *p);
-/* kernels the last time step launched: 1 = fused single-sweep kernel, 2 = the two passes */
+/* kernels the last time step launched: 1 = fused single-sweep kernel, 2 = the two passes (one more
+ * when a source illumination sum is attached and the step kernel does not accumulate it itself) */
 int WFD_Prop_StepKernels(void *p);
+/* Source illumination fused into the time step: with a device sum attached (ncells floats), every
+ * later step adds pCur^2 (the field the step reads) to it, as illum_accumulate_float would; the 3D
+ * Iso step kernel does it in place of a separate pass. NULL detaches. */
+int WFD_Prop_SetIllumination(void *p, float *accum);
 /* nsteps time steps of the object (TimeStep, then injection into pCur at time index it, then
  * extraction of pCur at it, it = it0, it0+1, ...; either table may be NULL), with every pair of steps
  * replayed from one CUDA graph when use_graph != 0; indices beyond nt are skipped. Enqueued on the

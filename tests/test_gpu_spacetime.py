@@ -258,3 +258,32 @@ def test_prop_run_matches_stepping(lib, name, shape, use_graph):
     for k in fa:
         assert np.array_equal(fa[k], fb[k]), (k, mismatch_report(fa[k], fb[k]))
     assert np.array_equal(ta, tb)
+
+
+@pytest.mark.parametrize("name,shape", [("Prop3DAcoIsoDenQ_DEO2_FDTD", (36, 21, 30)),
+                                        ("Prop3DAcoIsoDenQ_DEO2_FDTD", (37, 21, 30)),
+                                        ("Prop3DAcoVTIDenQ_DEO2_FDTD", (28, 22, 24)),
+                                        ("Prop2DAcoIsoDenQ_DEO2_FDTD", (44, 1, 38))])
+def test_illumination_fused_into_step(lib, name, shape):
+    """WFD_Prop_SetIllumination: every step adds pCur^2 (the field it reads) to the sum, inside the 3D Iso
+    step kernel (nz % 4 == 0) or as a separate pass otherwise; bitwise against float32 numpy."""
+    import torch
+    from tests.harness import ABIRunner, make_model
+    from wavefd_b200.abi import PROPAGATORS
+    ndim, physics = PROPAGATORS[name][:2]
+    g = ABIRunner(lib, name, shape, fs=True)
+    g.load(make_model(ndim, physics, shape, seed=6))
+    n = int(np.prod(shape))
+    acc = torch.zeros(n, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.WFD_Prop_SetIllumination(ctypes.c_void_p(g.p), ctypes.c_void_p(acc.data_ptr())) == 0
+    want = np.zeros(n, np.float32)
+    for _ in range(4):
+        pc = g.arr("PCur").reshape(-1).copy()
+        want = want + pc * pc  # float32: one rounding per operation
+        g.abi.TimeStep(g.p)
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(g.p)) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(acc.cpu().numpy(), want)
+    assert lib.WFD_Prop_SetIllumination(ctypes.c_void_p(g.p), None) == 0
+    g.close()

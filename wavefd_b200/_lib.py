@@ -55,6 +55,7 @@ def _declare(lib):
     fn("WFD_Points_Groups", c_long, [c_void_p])
     fn("WFD_Inject", c_int, [c_void_p, c_void_p, c_void_p, c_long, c_long, c_void_p])
     fn("WFD_Extract", c_int, [c_void_p, c_void_p, c_void_p, c_long, c_long, c_void_p])
+    fn("WFD_Prop_SetIllumination", c_int, [c_void_p, c_void_p])
     fn("WFD_Prop_Run", c_int, [c_void_p, c_long, c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_long, c_int])
     fn("WFD_IllumAccumulate", c_int, [c_void_p, c_void_p, c_long, c_void_p])
     fn("WFD_Interp", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_long, c_long, c_long, c_long, c_void_p])

@@ -65,3 +65,10 @@ extern "C" int WFD_Prop_Prefetch(void *p) {
 extern "C" void *WFD_Prop_Stream(void *p) { return p ? (void *)P(p)->stream : nullptr; }
 
 extern "C" int WFD_Prop_StepKernels(void *p) { return p ? P(p)->step_kernels : WFD_ERR_ARG; }
+
+extern "C" int WFD_Prop_SetIllumination(void *p, float *accum) {
+    if (!p) return WFD_ERR_ARG;
+    if (accum && !wfd::device_accessible(accum)) return WFD_ERR_ARG;
+    P(p)->illum = accum;
+    return WFD_OK;
+}

@@ -4,20 +4,22 @@
 namespace WFD_NS {
 using namespace wfd;
 
-bool fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
+int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
+    Fields Fn = F;
+    Fn.illum = nullptr;  // only the TMA-staged Iso kernel accumulates the illumination itself
     if (g.ndim == 3 && phys == ISO) {
         // TMA-staged kernel when the tensor maps can be encoded (nz*4 a multiple of 16 bytes),
         // else the variant that stages its tiles with ordinary loads
-        if (fused_iso3d_tma(g, F, s)) return true;
-        return fused_iso3d(g, F, s);
+        if (fused_iso3d_tma(g, F, s)) return F.illum ? 2 : 1;
+        return fused_iso3d(g, Fn, s) ? 1 : 0;
     }
     if (g.ndim == 3 && phys == VTI) {
         // the VTI kernel with x-direction register queues, else the ring-staged kernel TTI uses
-        if (fused_vti3d_tma(g, linear, F, s)) return true;
-        return fused_aniso3d_tma(g, phys, linear, F, s);
+        if (fused_vti3d_tma(g, linear, Fn, s)) return 1;
+        return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
     }
-    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, F, s);
-    return false;
+    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
+    return 0;
 }
 
 // timeout flags of every fused kernel, cleared on read

@@ -18,7 +18,8 @@
 // selects), edge tiles (selects), and the top tile with a free surface (selects plus the image
 // stencils above kz = 0, which only the first z quad needs).
 // Persistent CTAs loop over (tile, x-chunk) items; a chunk starts with 14 warm-up planes that only
-// fill the queues. Waits are bounded; on timeout the kernel records an error in a device status
+// fill the queues. With an illumination sum attached (single objects), each cell's pCur^2 is added
+// to it as the cell is updated. Waits are bounded; on timeout the kernel records an error in a device status
 // word and leaves. Requires nz % 4 == 0 (TMA row pitch); the caller falls back otherwise.
 #include "wfd_kernels.h"
 #include "wfd_tma.cuh"
@@ -156,7 +157,8 @@ template <int MODE>
 __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const bool xin, const bool top, const int z,
                                           const int y,
                                           const int zq, const int row, const float *sx, const float *pc,
-                                          const float *st, const float *TYs, const float *TZs, float *po, float *ps) {
+                                          const float *st, const float *TYs, const float *TZs, float *po, float *ps,
+                                          float *illum) {
     const int o = row * TZ + 4 * zq;
     const float4 pold4 = ld4(st + S_PO + o), v4 = ld4(st + S_V + o), q4 = ld4(st + S_Q + o);
     const float4 b4 = ld4(st + S_BH + (4 + row) * BZW + 4 + 4 * zq);
@@ -209,6 +211,16 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
     const long k = j * g.sx + (long)y * g.nz + z;
     st4(po + k, make_float4(npo[0], npo[1], npo[2], npo[3]));
     st4(ps + k, make_float4(nps[0], nps[1], nps[2], nps[3]));
+    if (illum) {
+        // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add, as
+        // illumination.c:31-53 does)
+        float4 a = ld4(illum + k);
+        a.x = __fadd_rn(a.x, __fmul_rn(pc[0], pc[0]));
+        a.y = __fadd_rn(a.y, __fmul_rn(pc[1], pc[1]));
+        a.z = __fadd_rn(a.z, __fmul_rn(pc[2], pc[2]));
+        a.w = __fadd_rn(a.w, __fmul_rn(pc[3], pc[3]));
+        st4(illum + k, a);
+    }
 }
 
 // Queue update of phase PH = q & 7: pCur(j+7) enters slot (PH+7)&7, the pass-1 x output at plane
@@ -388,7 +400,7 @@ __global__ void __launch_bounds__(NT, 3)
                 ext_stage<EDGE>(g, xin, tile_top, z0, y0, st, TYs, TZs);
                 __syncthreads();
                 if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, zq, row, sx, pc, st, TYs, TZs, out_pold,
-                                          out_pspace);
+                                          out_pspace, BATCH ? nullptr : F.illum);
             }
             __syncthreads();
             if (*abort_flag) {

@@ -61,6 +61,11 @@ void dropin(T *accum, T *field, size_t n) {
 }
 
 }  // namespace
+
+void illum_accumulate(float *sum, const float *field, long n, cudaStream_t s) {
+    if (n > 0) k_illum<float><<<blocks(n), 256, 0, s>>>(sum, const_cast<float *>(field), n);
+}
+
 }  // namespace wfd
 
 // ---- drop-in libillumination exports (illumination.c:3-53) ------------------------------------------

@@ -14,6 +14,7 @@ namespace wfd {
 struct Fields {
     float *v, *b, *q, *eps, *eta, *f, *st, *ct, *sp, *cp;
     float *pcur, *pold, *pspace, *mcur, *mold, *mspace;
+    float *illum;  // source illumination sum (sum over steps of pCur^2), or nullptr
 };
 
 // Scratch of the unfused passes (the reference's tmp arrays), device memory.
@@ -58,8 +59,9 @@ struct TileInfo {
     void pass1(const wfd::Grid &g, int phys, const wfd::Fields &F, const wfd::Scratch &S, cudaStream_t s); \
     void pass2(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, const wfd::Scratch &S,    \
                cudaStream_t s);                                                                          \
-    /* fused single-sweep steps; return false when the geometry is not handled */                        \
-    bool fused_step(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);     \
+    /* fused single-sweep steps; 0 when the geometry is not handled, 1 when stepped, 2 when stepped  \
+       with F.illum accumulated inside the step kernel */                                               \
+    int fused_step(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);      \
     void scale(const wfd::Grid &g, const wfd::Fields &F, bool two, cudaStream_t s);                      \
     void dplus(const wfd::Grid &g, const float *in, float *ox, float *oy, float *oz, cudaStream_t s);    \
     void dplus3(const wfd::Grid &g, const float *inx, const float *iny, const float *inz, float *ox,     \

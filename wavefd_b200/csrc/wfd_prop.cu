@@ -97,6 +97,7 @@ Fields Prop::fields() const {
     F.mcur = field[F_MCUR];
     F.mold = field[F_MOLD];
     F.mspace = field[F_MSPACE];
+    F.illum = illum;
     return F;
 }
 
@@ -278,10 +279,12 @@ int prop_sync(Prop *p) {
 int prop_step(Prop *p, bool linear, bool sync) {
     Grid g = p->grid();
     Fields F = p->fields();
-    bool done = false;
+    bool done = false, illum_done = false;
     if (p->fused) {
-        done = p->strict ? wfd_strict::fused_step(g, p->phys, linear, F, p->stream)
-                         : wfd_fast::fused_step(g, p->phys, linear, F, p->stream);
+        const int r = p->strict ? wfd_strict::fused_step(g, p->phys, linear, F, p->stream)
+                                : wfd_fast::fused_step(g, p->phys, linear, F, p->stream);
+        done = r > 0;
+        illum_done = r == 2;
     }
     if (!done) {
         if (!ensure_scratch(p, p->phys == ISO ? 3 : 6)) return p->status;
@@ -294,7 +297,9 @@ int prop_step(Prop *p, bool linear, bool sync) {
             wfd_fast::pass2(g, p->phys, linear, F, S, p->stream);
         }
     }
-    p->step_kernels = done ? 1 : 2;
+    // the illumination of pCur (read-only during the step) when the step kernel did not add it
+    if (p->illum && !illum_done) illum_accumulate(p->illum, p->field[F_PCUR], p->ncells(), p->stream);
+    p->step_kernels = (done ? 1 : 2) + (p->illum && !illum_done ? 1 : 0);
     if (int rc = check_cuda(p, cudaGetLastError(), "time step launch")) return rc;
     // pointer swap (prop3DAcoIsoDenQ_DEO2_FDTD.h:258-260)
     std::swap(p->field[F_PCUR], p->field[F_POLD]);

@@ -33,6 +33,7 @@ struct Prop {
     float *field[F_COUNT] = {};
     float *tmp[12] = {};     // scratch of the unfused passes (the reference's tmp arrays)
     float2 *work = nullptr;  // FFT workspace of the wavefield-separation condition
+    float *illum = nullptr;  // caller's source illumination sum (device), accumulated by every step
     long work_cols = 0;
     int status = WFD_OK;
     std::string message;
@@ -70,6 +71,9 @@ void apply_dplus2d(bool fs, long nx, long nz, float c1, float c2, float c3, floa
 // device call on this thread
 void prefetch_to_device(Prop *p, cudaStream_t s);
 bool take_host_touched();
+
+// sum[i] += field[i]^2 on the device (wfd_illum.cu)
+void illum_accumulate(float *sum, const float *field, long n, cudaStream_t s);
 
 // true when the pointer can be dereferenced by kernels (device or managed memory)
 bool device_accessible(const void *ptr);
