@@ -65,19 +65,23 @@ __device__ unsigned int d_status;
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
 __device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 #if WFD_STRICT
 // strict build: one rounded scalar operation per lane, never contracted (the reference has no FMA)
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return add2(mul2(a, b), c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+// a - b written as the reference's -b + a
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(neg2(b), a); }
 #else
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// Negation and subtraction as one packed instruction each: b * -1 is exact, so b * -1 + a rounds
+// once, like -b + a (a negated operand of the packed add would cost two scalar instructions).
+__device__ __forceinline__ float2 neg2(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 #endif
-// a - b written as the reference's -b + a
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(neg2(b), a); }
 __device__ __forceinline__ float2 sel2(bool c, float2 a, float2 b) { return c ? a : b; }
 __device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
 __device__ __forceinline__ float2 div2(float2 a, float2 b) { return make_float2(a.x / b.x, a.y / b.y); }
