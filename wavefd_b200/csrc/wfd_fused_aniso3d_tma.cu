@@ -55,6 +55,9 @@ constexpr int OFF_TZ = OFF_TY + 2 * TYR * TZ;
 constexpr int OFF_BAR = OFF_TZ + 2 * TY * TZW;
 constexpr size_t SMEM_BYTES = (size_t)OFF_BAR * 4 + (NR + NM) * 8 + 16;
 constexpr int WARMUP = 7;  // pass-1-only iterations before the first plane of a chunk
+// The thread that issues the TMA copies: lane 0 of warp 6, a warp without halo work (warps 0-5 do
+// the halo pairs), so that the issue does not lengthen the busiest warps' planes.
+constexpr int ISSUER = 192;
 static_assert((RBOX * 4) % 128 == 0 && (MBOX * 4) % 128 == 0 && (CBOX * 4) % 128 == 0, "TMA alignment");
 static_assert((OFF_MAT * 4) % 128 == 0 && (M_STAGE * 4) % 128 == 0, "TMA alignment");
 static_assert(OFF_BAR % 2 == 0, "mbarrier alignment");
@@ -160,7 +163,12 @@ __device__ __forceinline__ Out6 pass1(const Grid &g, const float *const (&ring)[
         dMy.x = 0.0f;
     }
     const int mo = er * MZW + ec;
-    const float2 bv = ld2(mat + MT_B * MBOX + mo), eps = ld2(mat + MT_E * MBOX + mo);
+    float2 bv = ld2(mat + MT_B * MBOX + mo);
+    const float2 eps = ld2(mat + MT_E * MBOX + mo);
+    // fast build, TTI: every output is a product with the buoyancy, so a zero buoyancy outside the
+    // reference's range zeroes all six (the derivatives and materials are finite: TMA fills zeros)
+    constexpr bool mask_b = !WFD_STRICT && PHYS == TTI;
+    if (mask_b) bv = sel2(ok, bv, bc2(0.0f));
     const float2 eta = ld2(mat + MT_A * MBOX + mo), fv = ld2(mat + MT_F * MBOX + mo);
     const float2 one = bc2(1.0f), two = bc2(2.0f);
     Out6 o;
@@ -205,13 +213,15 @@ __device__ __forceinline__ Out6 pass1(const Grid &g, const float *const (&ring)[
             o.mz = zero;
         }
     }
-    const float2 z2 = zero;
-    o.px = sel2(ok, o.px, z2);
-    o.py = sel2(ok, o.py, z2);
-    o.pz = sel2(ok, o.pz, z2);
-    o.mx = sel2(ok, o.mx, z2);
-    o.my = sel2(ok, o.my, z2);
-    o.mz = sel2(ok, o.mz, z2);
+    if (!mask_b) {
+        const float2 z2 = zero;
+        o.px = sel2(ok, o.px, z2);
+        o.py = sel2(ok, o.py, z2);
+        o.pz = sel2(ok, o.pz, z2);
+        o.mx = sel2(ok, o.mx, z2);
+        o.my = sel2(ok, o.my, z2);
+        o.mz = sel2(ok, o.mz, z2);
+    }
     return o;
 }
 
@@ -384,7 +394,7 @@ __global__ void __launch_bounds__(NT, 1)
             }
         };
 
-        if (tid == 0) {
+        if (tid == ISSUER) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             const int nr0 = nplanes < 8 + DR ? nplanes : 8 + DR;
             for (int rp = 0; rp < nr0; rp++) issue_ring(rp, r_issued + rp);
@@ -418,10 +428,15 @@ __global__ void __launch_bounds__(NT, 1)
         }
 
         bool stop = *abort_flag != 0;
+        // ring slot of plane q (the oldest of the eight in use) and slot/parity of plane q + 7, kept
+        // incrementally (no division by NR per plane)
+        unsigned rs0 = rseq % NR;
+        unsigned rw = (rseq + 7) % NR, rwpar = ((rseq + 7) / NR) & 1u;
+        const bool yz_tile = yok(g, y) && zok(g, z), yz_halo = yok(g, hy) && zok(g, hz);
         for (int q = 0; q < niter && !stop; q++) {
             const long j = jstart + q;
             const long P = j + 3;
-            if (tid == 0) {
+            if (tid == ISSUER) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 if (q + 8 + DR - 1 < nplanes && q >= 1) {
                     issue_ring(q + 8 + DR - 1, r_issued);
@@ -435,7 +450,7 @@ __global__ void __launch_bounds__(NT, 1)
             bool ok_w = true;
             if (q >= 1 && q + 7 < nplanes) {
                 const unsigned gi = rseq + q + 7;
-                ok_w = mbar_wait(&rbar[gi % NR], (gi / NR) & 1u);
+                ok_w = mbar_wait(&rbar[rw], rwpar);
                 if (ok_w) r_done = gi + 1;
                 if (top && ok_w) image_plane(gi);
             }
@@ -447,23 +462,24 @@ __global__ void __launch_bounds__(NT, 1)
                 atomicOr(&d_status, 1u);
             }
             const float *ring[8];
+            {
+                const float *r0 = sm + OFF_RING + rs0 * R_SLOT;
 #pragma unroll
-            for (int i = 0; i < 8; i++) ring[i] = sm + OFF_RING + ((rseq + q + i) % NR) * R_SLOT;
+                for (int i = 0; i < 8; i++) ring[i] = r0 + (rs0 + i >= NR ? (i - NR) * R_SLOT : i * R_SLOT);
+            }
             const float *mat = sm + OFF_MAT + (ms % NM) * M_STAGE;
             const bool pin = P >= 4 && P < g.nx - 4;
 
             // pass 1 at the lead plane: the tile pair, then the halo pair
-            const Out6 c = pass1<PHYS, 0>(g, ring, mat, row + 4, 4 + 2 * zp, pin && yok(g, y) && zok(g, z),
-                                          top && zp == 0);
+            const Out6 c = pass1<PHYS, 0>(g, ring, mat, row + 4, 4 + 2 * zp, pin && yz_tile, top && zp == 0);
             float2 h0 = bc2(0.0f), h1 = bc2(0.0f);
             // (the z-halo pairs above the free surface hold images, written by the tile pairs)
             if (h_kind == 1) {
-                const Out6 h = pass1<PHYS, 1>(g, ring, mat, h_er, h_ec, pin && yok(g, hy) && zok(g, hz),
-                                              top && zp == 0);
+                const Out6 h = pass1<PHYS, 1>(g, ring, mat, h_er, h_ec, pin && yz_halo, top && zp == 0);
                 h0 = h.py;
                 h1 = h.my;
             } else if (h_kind == 2 && !(top && h_ec < 4)) {
-                const Out6 h = pass1<PHYS, 2>(g, ring, mat, h_er, h_ec, pin && yok(g, hy) && zok(g, hz), false);
+                const Out6 h = pass1<PHYS, 2>(g, ring, mat, h_er, h_ec, pin && yz_halo, false);
                 h0 = h.pz;
                 h1 = h.mz;
             }
@@ -514,7 +530,7 @@ __global__ void __launch_bounds__(NT, 1)
                     const float2 sz = st8z(g, v, 0);
                     L[f] = fma2(bc2(g.idz), sz, fma2(bc2(g.idy), sy, mul2(bc2(g.idx), sx[f])));
                 }
-                const bool ok = j >= 4 && j < g.nx - 4 && yok(g, y) && zok(g, z);
+                const bool ok = j >= 4 && j < g.nx - 4 && yz_tile;
                 if (top && zp == 0) {  // free-surface row: every derivative is zero
                     L[0].x = 0.0f + 0.0f + 0.0f;
                     L[1].x = 0.0f + 0.0f + 0.0f;
@@ -535,12 +551,15 @@ __global__ void __launch_bounds__(NT, 1)
             }
             __syncthreads();
             if (*abort_flag) stop = true;
+            rs0 = rs0 + 1 == NR ? 0u : rs0 + 1;
+            rw = rw + 1 == NR ? 0u : rw + 1;
+            rwpar ^= rw == 0 ? 1u : 0u;
         }
         rseq += nplanes;
         mseq += niter;
         if (stop) break;
     }
-    if (*abort_flag && tid == 0) {
+    if (*abort_flag && tid == ISSUER) {
         for (unsigned gi = r_done; gi < r_issued; gi++) mbar_wait(&rbar[gi % NR], (gi / NR) & 1u, 100000000ull);
         for (unsigned gi = m_done; gi < m_issued; gi++) mbar_wait(&mbar[gi % NM], (gi / NM) & 1u, 100000000ull);
     }
