@@ -58,14 +58,47 @@ __device__ unsigned int d_status;
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float at(const float4 &v, int i) {
     return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
+// cells 0-1 (h = 0) or 2-3 (h = 1) of a quad
+__device__ __forceinline__ float2 half2(const float4 &v, int h) {
+    return h == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
+}
+#if WFD_STRICT
+// strict build: one rounded scalar operation per lane, never contracted (the reference has no FMA)
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return add2(mul2(a, b), c); }
+// a - b written as the reference's -b + a
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return add2(make_float2(-b.x, -b.y), a); }
+#else
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// b * -1 + a: one packed instruction, rounded once like -b + a
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+#endif
+__device__ __forceinline__ float2 div2(float2 a, float2 b) { return make_float2(a.x / b.x, a.y / b.y); }
+// lane-wise keep-or-replace by two bits of a cell mask
+__device__ __forceinline__ float2 keep2(unsigned mask, int bit, float2 v, float2 other) {
+    return make_float2((mask >> bit) & 1u ? v.x : other.x, (mask >> bit + 1) & 1u ? v.y : other.y);
+}
 
 // D+ at the centre of an 8-sample window w[0..7] = f(k-3..k+4); D- with w[0..7] = f(k-4..k+3)
+// (prop3DAcoIsoDenQ_DEO2_FDTD.h:846-864, :1113-1131), summed left to right
 __device__ __forceinline__ float st8(const Grid &g, float w0, float w1, float w2, float w3, float w4, float w5,
                                      float w6, float w7) {
     return g.c1 * (-w3 + w4) + g.c2 * (-w2 + w5) + g.c3 * (-w1 + w6) + g.c4 * (-w0 + w7);
+}
+// the same stencil on a pair of cells whose windows sit in the same lanes (x and y directions)
+__device__ __forceinline__ float2 st8p(const Grid &g, float2 w0, float2 w1, float2 w2, float2 w3, float2 w4,
+                                       float2 w5, float2 w6, float2 w7) {
+    float2 s = mul2(bc2(g.c1), sub2(w4, w3));
+    s = fma2(bc2(g.c2), sub2(w5, w2), s);
+    s = fma2(bc2(g.c3), sub2(w6, w1), s);
+    return fma2(bc2(g.c4), sub2(w7, w0), s);
 }
 
 // cells of the pass-1 outputs that the reference computes: interior, or free-surface rows 1..3
@@ -77,17 +110,52 @@ __device__ __forceinline__ bool xy_out_z(const Grid &g, int zz) {
 __device__ __forceinline__ bool z_out_z(const Grid &g, int zz) { return zz >= 0 && zz < g.nz - 4 && (zz >= 4 || g.fs); }
 __device__ __forceinline__ bool y_in(const Grid &g, int y) { return y >= 4 && y < g.ny - 4; }
 
-// pass-1 y/z outputs of the centre plane j into TYs/TZs
+// Thread tasks of the halo stage: threads 0-63 form the y outputs of 3 extended rows x 4 cells
+// (rows r0..r0+2, r0 = 3 (tid >> 3), columns 4 (tid & 7)..+3); threads 64-127 the z outputs of
+// 2-3 quads of one tile row (row (tid-64) >> 2, quads {0,1,2} {3,4,5} {6,7} {8,9} of the 10
+// extended-column quads at z0-4).
+__device__ __forceinline__ void ext_z_task(int tid, int &r, int &qa, int &nq) {
+    const int tt = tid - 64;
+    const int g4 = tt & 3;
+    r = tt >> 2;
+    qa = g4 == 0 ? 0 : (g4 == 1 ? 3 : (g4 == 2 ? 6 : 8));
+    nq = g4 < 2 ? 3 : 2;
+}
+// which of those cells the reference computes (given x): bit 4 rr + m (y task, row r0+rr, cell m)
+// or 4 k + m (z task, quad qa+k, cell m); fixed for an item
+__device__ __forceinline__ unsigned ext_mask(const Grid &g, int tid, int z0, int y0) {
+    unsigned mask = 0;
+    if (tid < 64) {
+        const int r0 = (tid >> 3) * 3, zz0 = z0 + 4 * (tid & 7);
+#pragma unroll
+        for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (y_in(g, y0 - 4 + r0 + rr) && xy_out_z(g, zz0 + m)) mask |= 1u << (4 * rr + m);
+    } else {
+        int r, qa, nq;
+        ext_z_task(tid, r, qa, nq);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (k < nq && y_in(g, y0 + r) && z_out_z(g, z0 - 4 + 4 * (qa + k) + m)) mask |= 1u << (4 * k + m);
+    }
+    return mask;
+}
+
+// pass-1 y/z outputs of the centre plane j into TYs/TZs (emask: ext_mask of this thread)
 template <int MODE>
-__device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const bool top, const int z0, const int y0,
-                                          const float *st, float *TYs, float *TZs) {
+__device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const bool top, const int z0,
+                                          const unsigned emask, const float *st, float *TYs, float *TZs) {
     const int tid = threadIdx.x;
     const float *Pc = st + S_PH;
     const float *Bc = st + S_BH;
+    const unsigned em = xin ? emask : 0u;
+    const float2 zero = bc2(0.0f);
     if (tid < 64) {
         const int zq = tid & 7;
         const int r0 = (tid >> 3) * 3;  // rows r0..r0+2 of the 24 extended rows
-        const int zz0 = z0 + 4 * zq;
         float4 w[10];
 #pragma unroll
         for (int i = 0; i < 10; i++)  // row 30 would only feed the unused padding row 23
@@ -95,28 +163,24 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const b
 #pragma unroll
         for (int rr = 0; rr < 3; rr++) {
             const int r = r0 + rr;
-            const bool rowok = xin && y_in(g, y0 - 4 + r);
             const float4 b = ld4(Bc + r * BZW + 4 + 4 * zq);
-            float out[4];
+            float2 out[2];
 #pragma unroll
-            for (int m = 0; m < 4; m++) {
-                const float s = st8(g, at(w[rr], m), at(w[rr + 1], m), at(w[rr + 2], m), at(w[rr + 3], m),
-                                    at(w[rr + 4], m), at(w[rr + 5], m), at(w[rr + 6], m), at(w[rr + 7], m));
-                float t = at(b, m) * (g.idy * s);
-                if (MODE != INNER) t = (rowok && xy_out_z(g, zz0 + m)) ? t : 0.0f;
-                out[m] = t;
+            for (int h = 0; h < 2; h++) {
+                const float2 s = st8p(g, half2(w[rr], h), half2(w[rr + 1], h), half2(w[rr + 2], h),
+                                      half2(w[rr + 3], h), half2(w[rr + 4], h), half2(w[rr + 5], h),
+                                      half2(w[rr + 6], h), half2(w[rr + 7], h));
+                float2 t = mul2(half2(b, h), mul2(bc2(g.idy), s));
+                if (MODE != INNER) t = keep2(em, 4 * rr + 2 * h, t, zero);
+                out[h] = t;
             }
-            st4(TYs + r * TZ + 4 * zq, make_float4(out[0], out[1], out[2], out[3]));
+            st4(TYs + r * TZ + 4 * zq, make_float4(out[0].x, out[0].y, out[1].x, out[1].y));
         }
     } else {
-        // 16 rows x 10 quads over 64 threads: 4 threads per row, quads {0,1,2} {3,4,5} {6,7} {8,9},
-        // each thread sliding along z over its contiguous quads
-        const int tt = tid - 64;
-        const int r = tt >> 2;
-        const int g4 = tt & 3;
-        const int qa = g4 == 0 ? 0 : (g4 == 1 ? 3 : (g4 == 2 ? 6 : 8));
-        const int nq = g4 < 2 ? 3 : 2;
-        const bool rowok = xin && y_in(g, y0 + r);
+        // each thread slides along z over its contiguous quads (scalar stencils: a pair of
+        // neighbouring z cells has its windows one lane apart)
+        int r, qa, nq;
+        ext_z_task(tid, r, qa, nq);
         const float *rowp = Pc + (r + 7) * PZW;
         float v[20];
 #pragma unroll
@@ -144,7 +208,7 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const b
                     s = st8(g, pm(m - 3), pm(m - 2), pm(m - 1), pm(m), pm(m + 1), pm(m + 2), pm(m + 3), pm(m + 4));
                 }
                 float t = at(b, m) * (g.idz * s);
-                if (MODE != INNER) t = (rowok && z_out_z(g, zb + m)) ? t : 0.0f;
+                if (MODE != INNER) t = ((em >> (4 * k + m)) & 1u) ? t : 0.0f;
                 out[m] = t;
             }
             st4(TZs + r * TZW + 4 * qi, make_float4(out[0], out[1], out[2], out[3]));
@@ -152,13 +216,13 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const b
     }
 }
 
-// D- in y and z, the time update and the stores of this thread's 4 cells
+// D- in y and z, the time update and the stores of this thread's 4 cells (fmask bit m: the
+// reference updates cell m, given x)
 template <int MODE>
 __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const bool xin, const bool top, const int z,
-                                          const int y,
-                                          const int zq, const int row, const float *sx, const float *pc,
-                                          const float *st, const float *TYs, const float *TZs, float *po, float *ps,
-                                          float *illum) {
+                                          const int y, const unsigned fmask, const int zq, const int row,
+                                          const float2 *sx, const float2 *pc, const float *st, const float *TYs,
+                                          const float *TZs, float *po, float *ps, float *illum) {
     const int o = row * TZ + 4 * zq;
     const float4 pold4 = ld4(st + S_PO + o), v4 = ld4(st + S_V + o), q4 = ld4(st + S_Q + o);
     const float4 b4 = ld4(st + S_BH + (4 + row) * BZW + 4 + 4 * zq);
@@ -168,84 +232,94 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
     const float *tzr = TZs + row * TZW;
     const float4 t0 = ld4(tzr + 4 * zq), t1 = ld4(tzr + 4 * zq + 4), t2 = ld4(tzr + 4 * zq + 8);
     const float w[12] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w, t2.x, t2.y, t2.z, t2.w};
-    const bool rowok = xin && y_in(g, y);
-    float npo[4], nps[4];
+    const unsigned fm = xin ? fmask : 0u;
+    float2 npo[2], nps[2];
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const float pcv = pc[m];
-        const float pov = at(pold4, m);
-        const float sy = st8(g, at(ty[0], m), at(ty[1], m), at(ty[2], m), at(ty[3], m), at(ty[4], m),
-                             at(ty[5], m), at(ty[6], m), at(ty[7], m));
-        float sz = st8(g, w[m], w[m + 1], w[m + 2], w[m + 3], w[m + 4], w[m + 5], w[m + 6], w[m + 7]);
-        float L = g.idx * sx[m] + g.idy * sy + g.idz * sz;
+    for (int h = 0; h < 2; h++) {
+        const int m0 = 2 * h;
+        const float2 sy = st8p(g, half2(ty[0], h), half2(ty[1], h), half2(ty[2], h), half2(ty[3], h),
+                               half2(ty[4], h), half2(ty[5], h), half2(ty[6], h), half2(ty[7], h));
+        const float2 sz = make_float2(
+            st8(g, w[m0], w[m0 + 1], w[m0 + 2], w[m0 + 3], w[m0 + 4], w[m0 + 5], w[m0 + 6], w[m0 + 7]),
+            st8(g, w[m0 + 1], w[m0 + 2], w[m0 + 3], w[m0 + 4], w[m0 + 5], w[m0 + 6], w[m0 + 7], w[m0 + 8]));
+#if WFD_STRICT
+        float2 L = add2(add2(mul2(bc2(g.idx), sx[h]), mul2(bc2(g.idy), sy)), mul2(bc2(g.idz), sz));
+#else
+        float2 L = fma2(bc2(g.idx), sx[h], fma2(bc2(g.idy), sy, mul2(bc2(g.idz), sz)));
+#endif
         if (top && z == 0) {
-            if (m == 0) {
-                L = 0.0f + 0.0f + 0.0f;  // the free surface row: all derivatives are zero
-            } else {
-                // symmetric image above the free surface, t[-j] = t[j-1]; column of z is z+4
-                auto tm = [&](int jz) { return tzr[(jz >= 0 ? jz : -jz - 1) + 4]; };
-                sz = st8(g, tm(m - 4), tm(m - 3), tm(m - 2), tm(m - 1), tm(m), tm(m + 1), tm(m + 2), tm(m + 3));
-                const float dx = g.idx * sx[m];
-                const float dy = g.idy * sy;
-                const float dz = g.idz * sz;
-                L = dx + dy + dz;
+            // the free surface row (cell 0): all derivatives are zero; cells 1-3: symmetric image
+            // above the free surface, t[-j] = t[j-1] (column of z is z+4)
+            float Ll[2] = {L.x, L.y};
+            const float sxl[2] = {sx[h].x, sx[h].y}, syl[2] = {sy.x, sy.y};
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int m = m0 + e;
+                if (m == 0) {
+                    Ll[e] = 0.0f + 0.0f + 0.0f;
+                } else {
+                    auto tm = [&](int jz) { return tzr[(jz >= 0 ? jz : -jz - 1) + 4]; };
+                    const float szi =
+                        st8(g, tm(m - 4), tm(m - 3), tm(m - 2), tm(m - 1), tm(m), tm(m + 1), tm(m + 2), tm(m + 3));
+                    const float dx = g.idx * sxl[e];
+                    const float dy = g.idy * syl[e];
+                    const float dz = g.idz * szi;
+                    Ll[e] = dx + dy + dz;
+                }
             }
-        } else if (WFD_STRICT) {
-            const float dx = g.idx * sx[m];
-            const float dy = g.idy * sy;
-            const float dz = g.idz * sz;
-            L = dx + dy + dz;
+            L = make_float2(Ll[0], Ll[1]);
         }
-        const float V = at(v4, m);
-        const float dt2V2_B = g.dt2 * V * V / at(b4, m);
-        float np = dt2V2_B * L - at(q4, m) * (pcv - pov) - pov + 2 * pcv;
-        float nl = L;
+        const float2 V = half2(v4, h), pcv = pc[h], pov = half2(pold4, h);
+        // dt^2 V^2 / B L - Q (pCur - pOld) - pOld + 2 pCur, left to right (:247-261)
+        const float2 k2 = div2(mul2(mul2(bc2(g.dt2), V), V), half2(b4, h));
+        const float2 t = sub2(sub2(mul2(k2, L), mul2(half2(q4, h), sub2(pcv, pov))), pov);
+        float2 np = add2(t, mul2(bc2(2.0f), pcv));
+        float2 nl = L;
         if (MODE != INNER) {
-            const bool ok = rowok && z_out_z(g, z + m);
-            np = ok ? np : pov;  // cells the reference leaves alone
-            nl = ok ? nl : 0.0f;
+            np = keep2(fm, m0, np, pov);  // cells the reference leaves alone
+            nl = keep2(fm, m0, nl, bc2(0.0f));
         }
-        npo[m] = np;
-        nps[m] = nl;
+        npo[h] = np;
+        nps[h] = nl;
     }
     const long k = j * g.sx + (long)y * g.nz + z;
-    st4(po + k, make_float4(npo[0], npo[1], npo[2], npo[3]));
-    st4(ps + k, make_float4(nps[0], nps[1], nps[2], nps[3]));
+    st4(po + k, make_float4(npo[0].x, npo[0].y, npo[1].x, npo[1].y));
+    st4(ps + k, make_float4(nps[0].x, nps[0].y, nps[1].x, nps[1].y));
     if (illum) {
         // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add, as
         // illumination.c:31-53 does)
         float4 a = ld4(illum + k);
-        a.x = __fadd_rn(a.x, __fmul_rn(pc[0], pc[0]));
-        a.y = __fadd_rn(a.y, __fmul_rn(pc[1], pc[1]));
-        a.z = __fadd_rn(a.z, __fmul_rn(pc[2], pc[2]));
-        a.w = __fadd_rn(a.w, __fmul_rn(pc[3], pc[3]));
+        a.x = __fadd_rn(a.x, __fmul_rn(pc[0].x, pc[0].x));
+        a.y = __fadd_rn(a.y, __fmul_rn(pc[0].y, pc[0].y));
+        a.z = __fadd_rn(a.z, __fmul_rn(pc[1].x, pc[1].x));
+        a.w = __fadd_rn(a.w, __fmul_rn(pc[1].y, pc[1].y));
         st4(illum + k, a);
     }
 }
 
 // Queue update of phase PH = q & 7: pCur(j+7) enters slot (PH+7)&7, the pass-1 x output at plane
-// j+3 enters qt slot (PH+7)&7; returns the D- x stencil at plane j and pCur(j).
+// j+3 enters qt slot (PH+7)&7; returns the D- x stencil at plane j and pCur(j). Queues hold the
+// quad as two cell pairs.
 template <int PH>
-__device__ __forceinline__ void queue_phase(float (&qp)[8][4], float (&qt)[8][4], const Grid &g, const bool xin_a,
-                                            const unsigned txmask, const float4 pn, const float4 bn, float *sx,
-                                            float *pc) {
+__device__ __forceinline__ void queue_phase(float2 (&qp)[8][2], float2 (&qt)[8][2], const Grid &g, const bool xin_a,
+                                            const unsigned txmask, const float4 pn, const float4 bn, float2 *sx,
+                                            float2 *pc) {
     constexpr int N = (PH + 7) & 7;
-    qp[N][0] = pn.x;
-    qp[N][1] = pn.y;
-    qp[N][2] = pn.z;
-    qp[N][3] = pn.w;
+    qp[N][0] = half2(pn, 0);
+    qp[N][1] = half2(pn, 1);
+    const unsigned tm = xin_a ? txmask : 0u;
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const float s = st8(g, qp[(PH + 0) & 7][m], qp[(PH + 1) & 7][m], qp[(PH + 2) & 7][m], qp[(PH + 3) & 7][m],
-                            qp[(PH + 4) & 7][m], qp[(PH + 5) & 7][m], qp[(PH + 6) & 7][m], qp[N][m]);
-        const float t = at(bn, m) * (g.idx * s);
-        qt[N][m] = (xin_a && ((txmask >> m) & 1u)) ? t : 0.0f;
+    for (int h = 0; h < 2; h++) {
+        const float2 s = st8p(g, qp[(PH + 0) & 7][h], qp[(PH + 1) & 7][h], qp[(PH + 2) & 7][h], qp[(PH + 3) & 7][h],
+                              qp[(PH + 4) & 7][h], qp[(PH + 5) & 7][h], qp[(PH + 6) & 7][h], qp[N][h]);
+        const float2 t = mul2(half2(bn, h), mul2(bc2(g.idx), s));
+        qt[N][h] = keep2(tm, 2 * h, t, bc2(0.0f));
     }
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        sx[m] = st8(g, qt[(PH + 0) & 7][m], qt[(PH + 1) & 7][m], qt[(PH + 2) & 7][m], qt[(PH + 3) & 7][m],
-                    qt[(PH + 4) & 7][m], qt[(PH + 5) & 7][m], qt[(PH + 6) & 7][m], qt[N][m]);
-        pc[m] = qp[PH][m];
+    for (int h = 0; h < 2; h++) {
+        sx[h] = st8p(g, qt[(PH + 0) & 7][h], qt[(PH + 1) & 7][h], qt[(PH + 2) & 7][h], qt[(PH + 3) & 7][h],
+                     qt[(PH + 4) & 7][h], qt[(PH + 5) & 7][h], qt[(PH + 6) & 7][h], qt[N][h]);
+        pc[h] = qp[PH][h];
     }
 }
 
@@ -328,13 +402,15 @@ __global__ void __launch_bounds__(NT, 3)
         const long xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
         const long jstart = xbeg - WARMUP;
         const int ngroups = (int)(xend - jstart);
-        // the tile and its halo of extended rows/columns lie inside [4, n-4) in y and z
-        const bool tile_inner = z0 - 4 >= 4 && z0 + TZ + 4 <= g.nz - 4 && y0 - 4 >= 4 && y0 + TY + 4 <= g.ny - 4;
         const bool tile_top = z0 == 0 && g.fs;
         unsigned txmask = 0;  // cells of this thread whose pass-1 x output is computed (given x)
+        unsigned fmask = 0;   // cells of this thread that are updated (given x)
 #pragma unroll
-        for (int m = 0; m < 4; m++)
+        for (int m = 0; m < 4; m++) {
             if (y_in(g, y) && xy_out_z(g, z + m)) txmask |= 1u << m;
+            if (y_in(g, y) && z_out_z(g, z + m)) fmask |= 1u << m;
+        }
+        const unsigned emask = ext_mask(g, tid, z0, y0);
 
         auto issue = [&](long jj, unsigned gs) {
             uint64_t *bar = &bars[gs % NS];
@@ -354,14 +430,15 @@ __global__ void __launch_bounds__(NT, 3)
             out_to = gseq + (D < ngroups ? D : ngroups);
         }
         // queues: qp[(q+i)&7] = pCur(j+i), qt[(q+i)&7] = pass-1 x output at plane j-4+i
-        float qp[8][4], qt[8][4];
+        float2 qp[8][2], qt[8][2];
 #pragma unroll
         for (int i = 0; i < 8; i++)
 #pragma unroll
-            for (int m = 0; m < 4; m++) {
-                qp[i][m] = 0.0f;
-                qt[i][m] = 0.0f;
+            for (int h = 0; h < 2; h++) {
+                qp[i][h] = bc2(0.0f);
+                qt[i][h] = bc2(0.0f);
             }
+        unsigned slot = gseq % NS, par = (gseq / NS) & 1u;  // stage and phase of group gseq + q
 
         bool stop = false;
         for (int q = 0; q < ngroups; q++) {
@@ -371,13 +448,15 @@ __global__ void __launch_bounds__(NT, 3)
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
             }
-            if (!mbar_wait(&bars[gs % NS], (gs / NS) & 1u)) {
+            if (!mbar_wait(&bars[slot], par)) {
                 atomicExch(abort_flag, 1);
                 atomicOr(&d_status, 1u);
             }
             if (tid == 0) out_from = gs + 1;
-            const float *st = sm + (gs % NS) * STAGE;
-            float sx[4], pc[4];
+            const float *st = sm + slot * STAGE;
+            slot = slot + 1 == NS ? 0u : slot + 1;
+            par ^= slot == 0 ? 1u : 0u;
+            float2 sx[2], pc[2];
             {
                 const int o = row * TZ + 4 * zq;
                 const float4 pn = ld4(st + S_PN + o);
@@ -397,9 +476,9 @@ __global__ void __launch_bounds__(NT, 3)
             if (j >= xbeg) {
                 const bool xin = j >= 4 && j < g.nx - 4;
                 // one code path for every tile (the selects are cheap, code size is not)
-                ext_stage<EDGE>(g, xin, tile_top, z0, y0, st, TYs, TZs);
+                ext_stage<EDGE>(g, xin, tile_top, z0, emask, st, TYs, TZs);
                 __syncthreads();
-                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, zq, row, sx, pc, st, TYs, TZs, out_pold,
+                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, fmask, zq, row, sx, pc, st, TYs, TZs, out_pold,
                                           out_pspace, BATCH ? nullptr : F.illum);
             }
             __syncthreads();
