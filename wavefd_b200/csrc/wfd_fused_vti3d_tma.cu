@@ -12,9 +12,9 @@
 //   z0-4, y0-4); pCur(j+7), mCur(j+7); b, eps, f (j+3); pOld, mOld, V, Q (j)  (32 x 16 each).
 // A thread owns a pair of consecutive z cells of one row and keeps, per field, a register queue of
 // pCur (planes j..j+7) and of the pass-1 x output (planes j-4..j+3); slot = plane mod 8, one code
-// path per phase. The pass-1 y outputs of plane j on the 24 halo-extended rows (threads 0-127, one
-// field, one quad, three rows sliding along y) and the z outputs on the 40 extended columns (threads
-// 128-255, both fields, one quad per task, 160 tasks) go to shared memory; then every thread applies D- and the time
+// path per phase. The pass-1 y outputs of plane j on the 24 halo-extended rows (threads 0-95, one
+// field, one quad, four rows sliding along y) and the z outputs on the 40 extended columns (threads
+// 96-255, both fields, one quad each) go to shared memory; then every thread applies D- and the time
 // update to its pair and stores pOld, mOld (and pSpace, mSpace). Arithmetic on float2 pairs with
 // the packed FP32 instructions; the strict build uses separate IEEE multiply and add in the
 // reference's order (bitwise equal to the reference). Region rules are selects; the free-surface
@@ -111,21 +111,46 @@ __device__ __forceinline__ bool xy_out_z(const Grid &g, int z) { return z < g.nz
 // cells of the pass-1 z output and of the update
 __device__ __forceinline__ bool z_out_z(const Grid &g, int z) { return z >= 0 && z < g.nz - 4 && (z >= 4 || g.fs); }
 
-// pass-1 y outputs of one field (`f`) on 3 extended rows r0..r0+2 (y = y0-4+r) and one quad zq of
-// the centre plane, the 10-row window sliding along y: P: b*(1+2eps)*dy p; M: b*(1-f)*dy m
-__device__ __forceinline__ void ext_y(const Grid &g, const bool xin, const int y0, const int z0, const int f,
-                                      const int zq, const int r0, const float *st, float *TYs) {
+// Halo tasks of a plane: threads 0-95 form the pass-1 y outputs of one field on 4 extended rows
+// and one quad (f = tid / 48; rows 4 ((tid % 48) >> 3) ..+3 of the 24 extended rows, quad tid & 7);
+// threads 96-255 the z outputs of both fields on one tile row and one of the 10 extended-column
+// quads (row (tid-96) / 10, quad (tid-96) % 10). Which cells the reference computes depends on x
+// only through one flag, so the rest is a mask fixed for an item: bit 4 rr + m (y task, row
+// r0+rr, cell m) or m (z task, cell m).
+__device__ __forceinline__ unsigned ext_mask(const Grid &g, int tid, int z0, int y0) {
+    unsigned mask = 0;
+    if (tid < 96) {
+        const int t = tid % 48, zz0 = z0 + 4 * (t & 7), r0 = (t >> 3) * 4;
+#pragma unroll
+        for (int rr = 0; rr < 4; rr++)
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (y_in(g, y0 - 4 + r0 + rr) && xy_out_z(g, zz0 + m)) mask |= 1u << (4 * rr + m);
+    } else {
+        const int t = tid - 96, r = t / 10, zb = z0 - 4 + 4 * (t % 10);
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (y_in(g, y0 + r) && z_out_z(g, zb + m)) mask |= 1u << m;
+    }
+    return mask;
+}
+__device__ __forceinline__ float2 keep2(unsigned mask, int bit, float2 v) {
+    return make_float2((mask >> bit) & 1u ? v.x : 0.0f, (mask >> bit + 1) & 1u ? v.y : 0.0f);
+}
+
+// pass-1 y outputs of one field (`f`) on 4 extended rows r0..r0+3 (y = y0-4+r) and one quad zq of
+// the centre plane, the 8-row window sliding along y: P: b*(1+2eps)*dy p; M: b*(1-f)*dy m
+__device__ __forceinline__ void ext_y(const Grid &g, const unsigned em, const int f, const int zq, const int r0,
+                                      const float *st, float *TYs) {
     const float *Fc = st + (f == 0 ? S_PH : S_MH);
-    float4 w[10];
+    float4 w[11];
 #pragma unroll
     for (int i = 0; i < 8; i++) w[i] = ld4(Fc + (r0 + i) * PZW + 8 + 4 * zq);
-    const int zz0 = z0 + 4 * zq;
 #pragma unroll
-    for (int rr = 0; rr < 3; rr++) {
+    for (int rr = 0; rr < 4; rr++) {
         const int r = r0 + rr;
         if (rr > 0)  // the window slides one row (row 30 would only feed the unused padding row 23)
             w[rr + 7] = r0 + rr + 7 < PYH ? ld4(Fc + (r0 + rr + 7) * PZW + 8 + 4 * zq) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const bool rowok = xin && y_in(g, y0 - 4 + r);
         const float4 b = ld4(st + S_BH + r * MZW + 4 + 4 * zq);
         const float4 e = ld4(st + (f == 0 ? S_EH : S_FH) + r * MZW + 4 + 4 * zq);
         float o[4];
@@ -143,9 +168,7 @@ __device__ __forceinline__ void ext_y(const Grid &g, const bool xin, const int y
             const float2 bv = make_float2(at(b, m), at(b, m + 1)), ev = make_float2(at(e, m), at(e, m + 1));
             // prop3DAcoVTIDenQ_DEO2_FDTD.h:945-957: b*E (E = 1 + 2 eps) for P, b*(1 - f) for M
             const float2 k = f == 0 ? mul2(bv, fma2(bc2(2.0f), ev, bc2(1.0f))) : mul2(bv, sub2(bc2(1.0f), ev));
-            float2 t = mul2(k, d);
-            t.x = (rowok && xy_out_z(g, zz0 + m)) ? t.x : 0.0f;
-            t.y = (rowok && xy_out_z(g, zz0 + m + 1)) ? t.y : 0.0f;
+            const float2 t = keep2(em, 4 * rr + m, mul2(k, d));
             o[m] = t.x;
             o[m + 1] = t.y;
         }
@@ -156,11 +179,9 @@ __device__ __forceinline__ void ext_y(const Grid &g, const bool xin, const int y
 // pass-1 z outputs of both fields on tile row r and extended quad qi (column 4*qi is z = z0-4+4*qi);
 // in the top tile the task of quad 1 also writes quad 0, the symmetric image t[-k] = t[k-1] above
 // the free surface, and the task of quad 0 does nothing.
-__device__ __forceinline__ void ext_z(const Grid &g, const bool xin, const bool top, const int y0, const int z0,
-                                      const int r, const int qi, const float *st, float *TZs) {
+__device__ __forceinline__ void ext_z(const Grid &g, const unsigned em, const bool top, const int r, const int qi,
+                                      const float *st, float *TZs) {
     if (top && qi == 0) return;
-    const bool rowok = xin && y_in(g, y0 + r);
-    const int zb = z0 - 4 + 4 * qi;
     const bool img = top && qi == 1;  // cells z = 0, 1, 2 reach above the free surface
     float d[2][4];                    // idz * D+z of p and m on the quad
 #pragma unroll
@@ -207,11 +228,11 @@ __device__ __forceinline__ void ext_z(const Grid &g, const bool xin, const bool 
         const float2 SA2 = sqrt2(sub2(one, mul2(eta, eta)));
         const float2 tp = fma2(mul2(bv, mul2(FA, SA2)), dMz, mul2(mul2(bv, sub2(one, FAA)), dPz));
         const float2 tm = fma2(mul2(bv, add2(sub2(one, fv), FAA)), dMz, mul2(mul2(mul2(mul2(bv, fv), eta), SA2), dPz));
-        const bool ok0 = rowok && z_out_z(g, zb + m), ok1 = rowok && z_out_z(g, zb + m + 1);
-        op[m] = ok0 ? tp.x : 0.0f;
-        op[m + 1] = ok1 ? tp.y : 0.0f;
-        om[m] = ok0 ? tm.x : 0.0f;
-        om[m + 1] = ok1 ? tm.y : 0.0f;
+        const float2 kp = keep2(em, m, tp), km = keep2(em, m, tm);
+        op[m] = kp.x;
+        op[m + 1] = kp.y;
+        om[m] = km.x;
+        om[m + 1] = km.y;
     }
     float *tp = TZs + r * TZW + 4 * qi, *tm = TZs + TY * TZW + r * TZW + 4 * qi;
     st4(tp, make_float4(op[0], op[1], op[2], op[3]));
@@ -322,6 +343,8 @@ __global__ void __launch_bounds__(NT, 2)
         const int ngroups = (int)(xend - jstart);
         const bool top = z0 == 0 && g.fs;
         const bool okxz0 = y_in(g, y) && xy_out_z(g, z), okxz1 = y_in(g, y) && xy_out_z(g, z + 1);
+        const bool okz0 = y_in(g, y) && z_out_z(g, z), okz1 = y_in(g, y) && z_out_z(g, z + 1);
+        const unsigned emask = ext_mask(g, tid, z0, y0);
 
         auto issue = [&](long jj, unsigned gs) {
             uint64_t *bar = &bars[gs % NS];
@@ -391,11 +414,13 @@ __global__ void __launch_bounds__(NT, 2)
             }
             if (j >= xbeg) {
                 const bool xin = j >= 4 && j < g.nx - 4;
-                if (tid < 128) {  // 2 fields x 8 row groups x 8 quads
-                    const int f = tid >> 6, t = tid & 63;
-                    ext_y(g, xin, y0, z0, f, t & 7, (t >> 3) * 3, st, TYs);
-                } else {  // 16 rows x 10 quads over 128 threads
-                    for (int t = tid - 128; t < TY * 10; t += 128) ext_z(g, xin, top, y0, z0, t / 10, t % 10, st, TZs);
+                const unsigned em = xin ? emask : 0u;
+                if (tid < 96) {  // 2 fields x 6 row groups x 8 quads
+                    const int f = tid / 48, t = tid % 48;
+                    ext_y(g, em, f, t & 7, (t >> 3) * 4, st, TYs);
+                } else {  // 16 rows x 10 quads
+                    const int t = tid - 96;
+                    ext_z(g, em, top, t / 10, t % 10, st, TZs);
                 }
                 __syncthreads();
                 if (own) {
@@ -423,8 +448,7 @@ __global__ void __launch_bounds__(NT, 2)
                         L[0].x = 0.0f + 0.0f + 0.0f;
                         L[1].x = 0.0f + 0.0f + 0.0f;
                     }
-                    const bool rowok = xin && y_in(g, y);
-                    const bool ok0 = rowok && z_out_z(g, z), ok1 = rowok && z_out_z(g, z + 1);
+                    const bool ok0 = xin && okz0, ok1 = xin && okz1;
                     const float2 V = ld2(st + S_V + o), Q = ld2(st + S_Q + o);
                     const float2 B = ld2(st + S_BH + (row + 4) * MZW + 4 + 2 * zp);
                     const float2 k2 = div2(mul2(mul2(bc2(g.dt2), V), V), B);
