@@ -377,48 +377,100 @@ __global__ void k_err_hist(long nb, const float *__restrict__ err, unsigned *__r
         if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
-// step 2 (one thread): the lowest bin T whose blocks, with every higher bin's, fit in cap; blocks
-// above T are all kept raw and ctl[1] = the slots left for blocks in bin T. Bin 0 (zero error) is
-// never kept.
-__global__ void k_err_threshold(const unsigned *__restrict__ hist, long cap, int *__restrict__ ctl) {
-    long used = 0;
-    int t = 2047;
-    for (; t > 0; t--) {
-        if (used + hist[t] > cap) break;
-        used += hist[t];
+// step 2 (one CTA of 1024 threads): with S(t) = the blocks in bins >= t, the threshold bin T is
+// the largest t >= 1 with S(t) > cap (0 if none); every block above T is kept raw and ctl[1] =
+// cap - S(T+1) slots are left for blocks in bin T. S is non-increasing, so T = #{t >= 1 : S(t) >
+// cap}. Thread i holds bins 2047-2i and 2046-2i; a prefix sum over threads is a suffix sum over
+// bins. Bin 0 (zero error) is never kept.
+__global__ void __launch_bounds__(1024) k_err_threshold(const unsigned *__restrict__ hist, long cap,
+                                                         int *__restrict__ ctl) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ int count;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int b0 = 2047 - 2 * t, b1 = b0 - 1;
+    const unsigned long long h0 = hist[b0], h1 = hist[b1];
+    unsigned long long x = h0 + h1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    ctl[0] = t;                                   // bins > t: raw
-    ctl[1] = t > 0 ? (int)(cap - used) : 0;       // slots for bin t
-    ctl[2] = 0;                                   // slots taken (step 3)
-    ctl[3] = 0;                                   // slots taken in bin t
+    if (t == 0) count = 0;
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned long long y = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        wsum[lane] = y;
+    }
+    __syncthreads();
+    const unsigned long long above = (wid ? wsum[wid - 1] : 0ull) + x - (h0 + h1);  // bins > b0
+    const unsigned long long s0 = above + h0, s1 = s0 + h1;                         // S(b0), S(b1)
+    const unsigned long long ucap = (unsigned long long)cap;
+    const int c = (b0 >= 1 && s0 > ucap ? 1 : 0) + (b1 >= 1 && s1 > ucap ? 1 : 0);
+    const int wc = __reduce_add_sync(0xffffffffu, (unsigned)c);
+    if (lane == 0 && wc) atomicAdd(&count, wc);
+    __syncthreads();
+    const int T = count;
+    // S(T+1): the blocks above the threshold bin (none when T = 2047)
+    unsigned long long used = 0;
+    bool mine = false;
+    if (T == 2047) mine = t == 0;
+    else if (b0 == T + 1) mine = true, used = s0;
+    else if (b1 == T + 1) mine = true, used = s1;
+    if (mine) {
+        ctl[0] = T;                                     // bins > T: raw
+        ctl[1] = T > 0 ? (int)(cap - (long)used) : 0;  // slots for bin T
+        ctl[2] = 0;                                     // slots taken (step 3)
+        ctl[3] = 0;                                     // slots taken in bin T
+    }
 }
 
-// step 3: assign raw slots and copy those blocks' cells (x, y, z order; zero outside the grid)
-__global__ void k_err_pick(Dims d, const float *__restrict__ f, const float *__restrict__ err, long cap,
-                           int *__restrict__ ctl, int *__restrict__ raw_id, float *__restrict__ raw) {
-    const long nb = (long)d.nbx * d.nby * d.nbz;
-    __shared__ int slot;
-    for (long b = blockIdx.x; b < nb; b += gridDim.x) {
-        if (threadIdx.x == 0) {
-            const int bin = (int)(__float_as_uint(err[b]) >> 20);
-            int s = -1;
-            if (bin > ctl[0]) s = atomicAdd(&ctl[2], 1);
-            else if (bin == ctl[0] && bin > 0 && atomicAdd(&ctl[3], 1) < ctl[1]) s = atomicAdd(&ctl[2], 1);
-            if (s >= cap) s = -1;
-            if (s >= 0) raw_id[s] = (int)b;
-            slot = s;
+// step 3: assign raw slots, one block per thread with warp-aggregated counters
+__global__ void k_err_pick(long nb, const float *__restrict__ err, long cap, int *__restrict__ ctl,
+                           int *__restrict__ raw_id) {
+    const int T = ctl[0], tslots = ctl[1];
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long base = (long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nb; base += stride) {
+        const long b = base + lane;
+        const int bin = b < nb ? (int)(__float_as_uint(err[b]) >> 20) : 0;
+        const bool hi = b < nb && bin > T;
+        const bool eq = b < nb && bin == T && bin > 0;
+        const unsigned meq = __ballot_sync(0xffffffffu, eq);
+        int ebase = 0;
+        if (meq) {
+            if (lane == 0) ebase = atomicAdd(&ctl[3], __popc(meq));
+            ebase = __shfl_sync(0xffffffffu, ebase, 0);
         }
-        __syncthreads();
-        const int s = slot;
-        if (s >= 0) {
-            const int bz = (int)(b % d.nbz), by = (int)((b / d.nbz) % d.nby), bx = (int)(b / ((long)d.nbz * d.nby));
-            for (int j = threadIdx.x; j < 512; j += blockDim.x) {
-                const int x = bx * 8 + (j >> 6), y = by * 8 + ((j >> 3) & 7), z = bz * 8 + (j & 7);
-                raw[(long)s * 512 + j] =
-                    (x < d.nx && y < d.ny && z < d.nz) ? f[((long)x * d.ny + y) * d.nz + z] : 0.0f;
-            }
+        const bool take = hi || (eq && ebase + __popc(meq & below) < tslots);
+        const unsigned mt = __ballot_sync(0xffffffffu, take);
+        if (mt) {
+            int sbase = 0;
+            if (lane == 0) sbase = atomicAdd(&ctl[2], __popc(mt));
+            sbase = __shfl_sync(0xffffffffu, sbase, 0);
+            const int sl = sbase + __popc(mt & below);
+            if (take && sl < cap) raw_id[sl] = (int)b;
         }
-        __syncthreads();
+    }
+}
+
+// step 4: copy the raw blocks' cells (x, y, z order; zero outside the grid), one CTA per block
+__global__ void k_raw_gather(Dims d, const float *__restrict__ f, const int *__restrict__ ctl, long cap,
+                             const int *__restrict__ raw_id, float *__restrict__ raw) {
+    const int nraw = ctl[2] < cap ? ctl[2] : (int)cap;
+    for (int s = blockIdx.x; s < nraw; s += gridDim.x) {
+        const long b = raw_id[s];
+        const int bz = (int)(b % d.nbz), by = (int)((b / d.nbz) % d.nby), bx = (int)(b / ((long)d.nbz * d.nby));
+        for (int j = threadIdx.x; j < 512; j += blockDim.x) {
+            const int x = bx * 8 + (j >> 6), y = by * 8 + ((j >> 3) & 7), z = bz * 8 + (j & 7);
+            raw[(long)s * 512 + j] = (x < d.nx && y < d.ny && z < d.nz) ? f[((long)x * d.ny + y) * d.nz + z] : 0.0f;
+        }
     }
 }
 
@@ -899,8 +951,9 @@ extern "C" int WFD_Codec_Encode(void *codec, const float *field, long nx, long n
     k_encode<<<grid, NTC, ENC_SMEM, st>>>(d, field, c->wb, c->w, scale, err, lat);
     const int gb = (int)((nb + 255) / 256 < 1184 ? (nb + 255) / 256 : 1184);
     k_err_hist<<<gb, 256, 0, st>>>(nb, err, hist);
-    k_err_threshold<<<1, 1, 0, st>>>(hist, cap, ctl);
-    k_err_pick<<<(unsigned)(nb < 4096 ? nb : 4096), 128, 0, st>>>(d, field, err, cap, ctl, raw_id, raw);
+    k_err_threshold<<<1, 1024, 0, st>>>(hist, cap, ctl);
+    k_err_pick<<<gb, 256, 0, st>>>(nb, err, cap, ctl, raw_id);
+    k_raw_gather<<<(unsigned)(cap < 1184 ? cap : 1184), 128, 0, st>>>(d, field, ctl, cap, raw_id, raw);
     return cuda_status(cudaGetLastError(), "WFD_Codec_Encode");
 }
 
