@@ -55,8 +55,9 @@ constexpr int OFF_TZ = OFF_TY + 2 * TYR * TZ;
 constexpr int OFF_BAR = OFF_TZ + 2 * TY * TZW;
 constexpr size_t SMEM_BYTES = (size_t)OFF_BAR * 4 + (NR + NM) * 8 + 16;
 constexpr int WARMUP = 7;  // pass-1-only iterations before the first plane of a chunk
-// The thread that issues the TMA copies: lane 0 of warp 6, a warp without halo work (warps 0-5 do
-// the halo pairs), so that the issue does not lengthen the busiest warps' planes.
+// The thread that issues the TMA copies: lane 0 of warp 6, a warp without halo work (warps 0-3 do
+// the y-halo pairs, 4-5 the z-halo pairs), so that the issue does not lengthen the busiest warps'
+// planes.
 constexpr int ISSUER = 192;
 static_assert((RBOX * 4) % 128 == 0 && (MBOX * 4) % 128 == 0 && (CBOX * 4) % 128 == 0, "TMA alignment");
 static_assert((OFF_MAT * 4) % 128 == 0 && (M_STAGE * 4) % 128 == 0, "TMA alignment");
@@ -288,8 +289,8 @@ __global__ void __launch_bounds__(NT, 1)
         h_er = hr < 4 ? hr : hr + 16;
         h_ec = 4 + 2 * zp;
         h_kind = 1;
-    } else if (tid < 176) {
-        const int u = tid - 112;
+    } else if (tid >= 128 && tid < 192) {  // (warps 4-5: a warp holds one kind of halo task)
+        const int u = tid - 128;
         const int hp = u & 3;
         h_er = 4 + (u >> 2);
         h_ec = hp < 2 ? 2 * hp : 36 + 2 * (hp - 2);

@@ -47,6 +47,9 @@ constexpr int S_PH = 0, S_MH = S_PH + PH_, S_BH = S_MH + PH_, S_EH = S_BH + MH_,
 constexpr unsigned GROUP_BYTES = 4u * STAGE;
 constexpr unsigned WARM_BYTES = 4u * 5 * OS;  // warm-up planes: pCur, mCur (j+7), b, eps, f (j+3)
 constexpr int WARMUP = 14;
+// The thread that issues the TMA copies: lane 0 of warp 7, a warp of halo z tasks (the lighter
+// kind), so that the issue does not lengthen the busiest warps' planes.
+constexpr int ISSUER = 224;
 constexpr int OFF_TY = NS * STAGE;              // [2][TYR][TZ]
 constexpr int OFF_TZ = OFF_TY + 2 * TYR * TZ;   // [2][TY][TZW]
 constexpr int OFF_BAR = OFF_TZ + 2 * TY * TZW;
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(NT, 2)
 
     const long total = (long)ntz0 * nty0 * nch0;
     unsigned gseq = 0;                  // groups consumed so far by this CTA
-    unsigned out_from = 0, out_to = 0;  // groups issued but not yet consumed (thread 0)
+    unsigned out_from = 0, out_to = 0;  // groups issued but not yet consumed (issuing thread)
     const int zp = tid & 15, row = tid >> 4;
 
     for (long wstat = blockIdx.x;; wstat += gridDim.x) {
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(NT, 2)
                 tma_load_3d(s + S_Q, maps + 14, bar, z0, y0, (int)jj);
             }
         };
-        if (tid == 0) {
+        if (tid == ISSUER) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             for (int q = 0; q < D && q < ngroups; q++) issue(jstart + q, gseq + q);
             out_from = gseq;
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(NT, 2)
         for (int q = 0; q < ngroups; q++) {
             const long j = jstart + q;
             const unsigned gs = gseq + q;
-            if (tid == 0 && q + D < ngroups) {
+            if (tid == ISSUER && q + D < ngroups) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(NT, 2)
                 atomicExch(abort_flag, 1);
                 atomicOr(&d_status, 1u);
             }
-            if (tid == 0) out_from = gs + 1;
+            if (tid == ISSUER) out_from = gs + 1;
             const float *st = sm + (gs % NS) * STAGE;
             float2 sx[2], pc[2];
             {
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(NT, 2)
         gseq += ngroups;
         if (stop) break;
     }
-    if (*abort_flag && tid == 0) {
+    if (*abort_flag && tid == ISSUER) {
         for (unsigned gs = out_from; gs < out_to; gs++) mbar_wait(&bars[gs % NS], (gs / NS) & 1u, 100000000ull);
     }
 }
