@@ -280,6 +280,7 @@ void illum_accumulate_double(double *field_ginsu_accum, double *field_ginsu, siz
 #define WFD_ERR_ARG 3
 #define WFD_ERR_UNSUPPORTED 4
 #define WFD_ERR_TIMEOUT 5
+#define WFD_ERR_IO 6
 
 /* last error of calls that have no object (alloc, spacetime), and of a given object */
 int WFD_LastError(void);
@@ -337,6 +338,31 @@ int WFD_ExtractInterp(void *table, float *coarse, const float *field, const floa
 /* Source illumination for the time loop: accum[i] += field[i]^2 on device arrays (the arithmetic of
  * illum_accumulate_float), asynchronous on `stream`. */
 int WFD_IllumAccumulate(float *accum, const float *field, long n, void *stream);
+
+/* Snapshot files: saved forward fields on disk with an offsets/lengths index, the role of
+ * Compressor/compressedwrite/compressedread! (src/compressedio.jl:1-137) for the plain FP32
+ * fallback and for codec codes. Layout: a header ("WFDSNAP1", version, flags, nfields, slot bytes,
+ * data offset, then per field offset and length, -1 = never written; a multiple of 4096 bytes)
+ * and field i's payload at data offset + i * slot (slot = max_bytes rounded up to 4096). Writes and
+ * reads of device arrays are stream-ordered and asynchronous (device staging, pinned staging, a
+ * worker thread doing pwrite/pread); a write's source may be overwritten as soon as later work on
+ * `stream` runs. I/O errors (short writes: "wrote X of Y bytes of field i in <path>") are
+ * WFD_ERR_IO, reported by the call that sees them (the next Write/Read/Sync/Close). */
+#define WFD_SNAP_READ 1   /* open an existing file (nfields, max_bytes come from its header) */
+#define WFD_SNAP_HOST 2   /* payloads are host memory: pwrite/pread only, no CUDA call */
+#define WFD_SNAP_DIRECT 4 /* O_DIRECT for payloads where the file system allows it */
+#define WFD_SNAP_CODEC 8  /* recorded in the header: the payloads are codec codes */
+void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, int flags);
+int WFD_Snap_Write(void *f, long ifield, const void *src, long nbytes, void *stream);
+/* start reading field ifield into a staging slot (a later Read of it only waits) */
+int WFD_Snap_Prefetch(void *f, long ifield);
+int WFD_Snap_Read(void *f, long ifield, void *dst, long nbytes, void *stream);
+long WFD_Snap_Length(void *f, long ifield);
+long WFD_Snap_NumFields(void *f);
+int WFD_Snap_Flags(void *f);
+/* wait for every transfer, then write the header (index) */
+int WFD_Snap_Sync(void *f);
+int WFD_Snap_Close(void *f);
 
 /* Batched shots (no counterpart in the reference, whose Ginsu is exported but not defined,
  * src/WaveFD.jl:52). A batch advances many 3D objects made by the *_alloc calls above (uneven sizes;

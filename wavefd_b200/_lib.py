@@ -58,6 +58,15 @@ def _declare(lib):
     fn("WFD_Prop_SetIllumination", c_int, [c_void_p, c_void_p])
     fn("WFD_Prop_Run", c_int, [c_void_p, c_long, c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_long, c_int])
     fn("WFD_IllumAccumulate", c_int, [c_void_p, c_void_p, c_long, c_void_p])
+    fn("WFD_Snap_Open", c_void_p, [ctypes.c_char_p, c_long, c_long, c_int])
+    fn("WFD_Snap_Write", c_int, [c_void_p, c_long, c_void_p, c_long, c_void_p])
+    fn("WFD_Snap_Prefetch", c_int, [c_void_p, c_long])
+    fn("WFD_Snap_Read", c_int, [c_void_p, c_long, c_void_p, c_long, c_void_p])
+    fn("WFD_Snap_Length", c_long, [c_void_p, c_long])
+    fn("WFD_Snap_NumFields", c_long, [c_void_p])
+    fn("WFD_Snap_Flags", c_int, [c_void_p])
+    fn("WFD_Snap_Sync", c_int, [c_void_p])
+    fn("WFD_Snap_Close", c_int, [c_void_p])
     fn("WFD_Interp", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_long, c_long, c_long, c_long, c_void_p])
     fn("WFD_ExtractInterp", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_long, c_long, c_long, c_long,
                                      c_void_p])

@@ -12,7 +12,10 @@ Snapshot stores:
   HostStore    -- uncompressed FP32 in pinned host memory, copies overlapped with the propagation
                   (device staging ring + a copy stream, prefetch one snapshot ahead); the store for
                   shots whose saved fields do not fit in device memory;
-  DeviceStore  -- uncompressed FP32 in device memory (exact reference for small shots).
+  DeviceStore  -- uncompressed FP32 in device memory (exact reference for small shots);
+  DiskStore    -- uncompressed FP32 in a snapshot file on disk (wavefd_b200/snapio.py: offsets/
+                  lengths index, staging and a worker thread in the library), the fallback when
+                  the saved fields fit neither in device nor in host memory.
 """
 from __future__ import annotations
 
@@ -152,6 +155,43 @@ class HostStore:
 
     def nbytes(self):
         return self.host.numel() * 4
+
+
+class DiskStore:
+    """Uncompressed snapshots in a snapshot file: field i of snapshot k is file field k * nfields + i.
+    A put writes (device staging on the propagation stream, so the next step may overwrite pSpace;
+    the disk write runs behind it); a get reads snapshot k into the store's device arrays on the
+    adjoint stream and starts reading snapshot k - 1 (the adjoint asks in decreasing order)."""
+
+    def __init__(self, shape, nsnap, nfields, path, direct=False, keep=False):
+        import torch
+        from .snapio import SnapshotFile
+        self.shape, self.nf, self.path, self.keep = tuple(shape), nfields, str(path), keep
+        self.field_bytes = int(np.prod(self.shape)) * 4
+        self.file = SnapshotFile(self.path, "w", nsnap * nfields, self.field_bytes, direct=direct)
+        self.out = [torch.empty(self.shape, device="cuda") for _ in range(nfields)]
+        self.nsnap = nsnap
+
+    def put(self, k, fields, stream):
+        for i, f in enumerate(fields):
+            self.file.write(k * self.nf + i, f, stream)
+
+    def get(self, k, stream):
+        for i in range(self.nf):
+            self.file.read(k * self.nf + i, self.out[i], stream)
+        if k - 1 >= 0:
+            for i in range(self.nf):
+                self.file.prefetch((k - 1) * self.nf + i)
+        return self.out
+
+    def nbytes(self):
+        return self.nsnap * self.nf * self.field_bytes
+
+    def close(self):
+        import os
+        self.file.close()
+        if not self.keep and os.path.exists(self.path):
+            os.remove(self.path)
 
 
 def make_shot(physics, shape, seed=0, d=10.0, dt=0.0005, nsponge=40, fpeak=12.0, nt=1000, nrec=(32, 32),
