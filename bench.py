@@ -677,7 +677,8 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
                      "kernel": "whole step (kernels of " + W["name"] + " + injection + extraction)",
                      "algorithmic_bytes_per_cell": W["bytes_per_cell"], "kernel_ms": round(ms / K, 5),
                      "peak_source": peak_src},
-        "gpu_launches": K * (lib.WFD_Prop_StepKernels(prop.p) + 3),
+        # per step: the step kernel(s), the injection, the extraction with the time-index advance
+        "gpu_launches": K * (lib.WFD_Prop_StepKernels(prop.p) + 2),
         "clocks": clk.summary(),
     }
     del traces, wav, d_wav, d_trc, h_trc, h_wav

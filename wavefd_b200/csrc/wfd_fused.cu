@@ -19,6 +19,7 @@ int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_
         return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
     }
     if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
+    if (g.ndim == 2 && phys == ISO) return fused_iso2d(g, Fn, s) ? 1 : 0;
     return 0;
 }
 

@@ -67,6 +67,7 @@ struct TileInfo {
     void dplus3(const wfd::Grid &g, const float *inx, const float *iny, const float *inz, float *ox,     \
                 float *oy, float *oz, cudaStream_t s);                                                   \
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
+    bool fused_iso2d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \

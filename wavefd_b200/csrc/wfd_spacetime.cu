@@ -91,7 +91,31 @@ __global__ void k_scatter_groups_devit(long ngroups, const long *__restrict__ ke
     *dst = acc;
 }
 
-__global__ void k_tick(long *it) { *it += 1; }
+// extraction at the device time index (as k_scatter_groups_devit, by receiver) followed by the
+// index's advance: every block reads the index first, counts itself done, and the last block to
+// finish writes index + 1 (and resets the count for the next launch); no block waits for another
+__global__ void k_extract_tick(long ngroups, const long *__restrict__ key, const long *__restrict__ start,
+                               const long *__restrict__ other, const float *__restrict__ c,
+                               const float *__restrict__ field, float *data, long nt, long *d_it,
+                               unsigned *done) {
+    const long gi = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long it = *d_it;
+    if (gi < ngroups && it >= 1 && it <= nt) {
+        float *dst = data + key[gi] * nt + (it - 1);
+        float acc = *dst;
+        for (long j = start[gi]; j < start[gi + 1]; j++) acc = add_rn(acc, mul_rn(c[j], field[other[j]]));
+        *dst = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+            *d_it = it + 1;
+            *done = 0u;
+            __threadfence();
+        }
+    }
+}
 
 template <class T>
 __global__ void k_gather(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
@@ -298,10 +322,14 @@ int run_step(Prop *p, DeviceTable *src, const float *wav, DeviceTable *rec, floa
         wfd::k_scatter_groups_devit<<<wfd::nb(src->t.ngroups), 256, 0, s>>>(
             src->t.ngroups, src->t.d_key, src->t.d_start, src->t.d_other, src->t.d_c, 0, pc, const_cast<float *>(wav),
             nt, d_it);
+    // extraction and the advance of the time index in one launch (d_it[1] counts finished blocks)
+    unsigned *done = reinterpret_cast<unsigned *>(d_it + 1);
     if (rec && rec->t.ngroups)
-        wfd::k_scatter_groups_devit<<<wfd::nb(rec->t.ngroups), 256, 0, s>>>(
-            rec->t.ngroups, rec->t.d_key, rec->t.d_start, rec->t.d_other, rec->t.d_c, 1, pc, trc, nt, d_it);
-    wfd::k_tick<<<1, 1, 0, s>>>(d_it);
+        wfd::k_extract_tick<<<wfd::nb(rec->t.ngroups), 256, 0, s>>>(rec->t.ngroups, rec->t.d_key, rec->t.d_start,
+                                                                    rec->t.d_other, rec->t.d_c, pc, trc, nt, d_it,
+                                                                    done);
+    else
+        wfd::k_extract_tick<<<1, 32, 0, s>>>(0, nullptr, nullptr, nullptr, nullptr, pc, trc, nt, d_it, done);
     return cudaGetLastError() == cudaSuccess ? WFD_OK : wfd::prop_fail(p, WFD_ERR_CUDA, "time loop launch");
 }
 
@@ -319,9 +347,11 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     if (!p->fused || p->ndim == 2 || p->nz % 4 != 0)
         if (!wfd::ensure_scratch(p, p->phys == wfd::ISO ? 3 : 6)) return p->status;
     long *d_it = nullptr;
-    if (cudaMallocAsync(&d_it, sizeof(long), s) != cudaSuccess)
+    // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch
+    if (cudaMallocAsync(&d_it, 2 * sizeof(long), s) != cudaSuccess)
         return wfd::prop_fail(p, WFD_ERR_ALLOC, "time index allocation failed");
-    cudaMemcpyAsync(d_it, &it0, sizeof(long), cudaMemcpyHostToDevice, s);
+    const long init[2] = {it0, 0};
+    cudaMemcpyAsync(d_it, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
     long done = 0;
     int rc = WFD_OK;
