@@ -19,7 +19,6 @@ using namespace wfd;
 namespace {
 
 constexpr int TX = 16, TZ = 32, NT = 256;
-static_assert(TZ == 32, "one z column per thread in the x-output and update sweeps");
 constexpr int PXH = TX + 14, PZW = TZ + 14;  // pCur box: rows x0-7 .., columns z0-7 ..
 constexpr int BXH = TX + 8, BZW = TZ + 8;    // B box: rows x0-4 .., columns z0-4 ..
 constexpr int T0H = TX + 7;                  // pass-1 x output: rows x0-4 .. x0+TX+2, columns z0 ..
@@ -44,7 +43,7 @@ __device__ __forceinline__ float stm(const Grid &g, const W &w) {
 
 // threads as 32 (z, fastest) x 8 (x); every shared-memory box is swept with compile-time trip counts
 constexpr int WZ = 32, WX = NT / WZ;
-static_assert(NT % WZ == 0, "thread layout");
+static_assert(NT % WZ == 0 && TZ % WZ == 0, "thread layout");
 
 __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     __shared__ float P[PXH][PZW];
@@ -85,16 +84,18 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     // pass 1, x output (B * idx * D+x pCur) on rows x0-4 .. x0+TX+2
 #pragma unroll
     for (int r = tx; r < T0H; r += WX) {
-        const int c = tz;  // TZ == WZ: one column per thread
-        const long x = x0 - 4 + r, z = z0 + c;
-        const int reg = region2(g, x, z);
-        float t = 0.0f;
-        if (reg) {
-            const int pr = r + 3, pc = c + 7;  // P row/column of (x, z)
-            const float dx = (reg == 2 && z == 0) ? 0.0f : g.idx * stp(g, [&](int j) { return P[pr + j][pc]; });
-            t = Bs[r][c + 4] * dx;
+#pragma unroll
+        for (int c = tz; c < TZ; c += WZ) {
+            const long x = x0 - 4 + r, z = z0 + c;
+            const int reg = region2(g, x, z);
+            float t = 0.0f;
+            if (reg) {
+                const int pr = r + 3, pc = c + 7;  // P row/column of (x, z)
+                const float dx = (reg == 2 && z == 0) ? 0.0f : g.idx * stp(g, [&](int j) { return P[pr + j][pc]; });
+                t = Bs[r][c + 4] * dx;
+            }
+            T0[r][c] = t;
         }
-        T0[r][c] = t;
     }
     // pass 1, z output (B * idz * D+z pCur, the image supplying kz < 0) on columns z0-4 .. z0+TZ+2
 #pragma unroll
@@ -128,26 +129,28 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     // pass 2: D-, the time update with Q, pSpace (.h:943)
 #pragma unroll
     for (int r = tx; r < TX; r += WX) {
-        const int c = tz;
-        const long x = x0 + r, z = z0 + c;
-        if (x >= nx || z >= nz) continue;
-        const long k = x * nz + z;
-        const int reg = region2(g, x, z);
-        if (!reg) {
-            F.pspace[k] = 0.0f;
-            continue;
+#pragma unroll
+        for (int c = tz; c < TZ; c += WZ) {
+            const long x = x0 + r, z = z0 + c;
+            if (x >= nx || z >= nz) continue;
+            const long k = x * nz + z;
+            const int reg = region2(g, x, z);
+            if (!reg) {
+                F.pspace[k] = 0.0f;
+                continue;
+            }
+            float dx = 0.0f, dz = 0.0f;
+            if (!(reg == 2 && z == 0)) {
+                dx = g.idx * stm(g, [&](int j) { return T0[r + 4 + j][c]; });
+                dz = g.idz * stm(g, [&](int j) { return T2[r][c + 4 + j]; });
+            }
+            const float L = dx + dz;
+            const float V = F.v[k];
+            const float dt2V2_B = g.dt2 * V * V / F.b[k];
+            const float pc = F.pcur[k], po = F.pold[k];
+            F.pold[k] = dt2V2_B * L - F.q[k] * (pc - po) - po + 2 * pc;
+            F.pspace[k] = L;
         }
-        float dx = 0.0f, dz = 0.0f;
-        if (!(reg == 2 && z == 0)) {
-            dx = g.idx * stm(g, [&](int j) { return T0[r + 4 + j][c]; });
-            dz = g.idz * stm(g, [&](int j) { return T2[r][c + 4 + j]; });
-        }
-        const float L = dx + dz;
-        const float V = F.v[k];
-        const float dt2V2_B = g.dt2 * V * V / F.b[k];
-        const float pc = F.pcur[k], po = F.pold[k];
-        F.pold[k] = dt2V2_B * L - F.q[k] * (pc - po) - po + 2 * pc;
-        F.pspace[k] = L;
     }
 }
 
