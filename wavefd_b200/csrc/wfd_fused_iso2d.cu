@@ -3,8 +3,9 @@
 // small (a 501 x 501 field is 1 MB and stays in L2), so a step is bound by launch latency, not by
 // bandwidth: one kernel instead of two (and no scratch arrays in global memory).
 //
-// A CTA of 256 threads owns a tile of TX x TZ cells (x rows, z contiguous). It loads pCur on the
-// tile plus 7 cells each side and B plus 4 each side into shared memory, forms the pass-1 x output
+// A CTA of 512 threads owns a tile of 16 x 64 cells (x rows, z contiguous; the fastest of the shapes
+// timed on a 501 x 501 grid: 8x32, 16x32, 32x32 and 16x64 cells, 256 or 512 threads). It loads pCur
+// on the tile plus 7 cells each side and B plus 4 each side into shared memory, forms the pass-1 x output
 // on rows x0-4 .. x0+TX+2 of the tile's columns and the z output on columns z0-4 .. z0+TZ+2 of its
 // rows (the halo is recomputed by each CTA, as neighbouring CTAs' pass-1 cells), then applies D- and
 // the update to its cells. Free surface: pCur above kz = 0 is its antisymmetric image (D+ input),
@@ -18,7 +19,7 @@ using namespace wfd;
 
 namespace {
 
-constexpr int TX = 16, TZ = 32, NT = 256;
+constexpr int TX = 16, TZ = 64, NT = 512;
 constexpr int PXH = TX + 14, PZW = TZ + 14;  // pCur box: rows x0-7 .., columns z0-7 ..
 constexpr int BXH = TX + 8, BZW = TZ + 8;    // B box: rows x0-4 .., columns z0-4 ..
 constexpr int T0H = TX + 7;                  // pass-1 x output: rows x0-4 .. x0+TX+2, columns z0 ..
@@ -41,7 +42,7 @@ __device__ __forceinline__ float stm(const Grid &g, const W &w) {
     return g.c1 * (-w(-1) + w(0)) + g.c2 * (-w(-2) + w(1)) + g.c3 * (-w(-3) + w(2)) + g.c4 * (-w(-4) + w(3));
 }
 
-// threads as 32 (z, fastest) x 8 (x); every shared-memory box is swept with compile-time trip counts
+// threads as 32 (z, fastest) x NT/32 (x); every shared-memory box is swept with compile-time trip counts
 constexpr int WZ = 32, WX = NT / WZ;
 static_assert(NT % WZ == 0 && TZ % WZ == 0, "thread layout");
 
