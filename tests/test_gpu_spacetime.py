@@ -260,6 +260,56 @@ def test_prop_run_matches_stepping(lib, name, shape, use_graph):
     assert np.array_equal(ta, tb)
 
 
+@pytest.mark.parametrize("nrec", [0, 600])
+def test_prop_run_index_advance(lib, nrec):
+    """The time index of WFD_Prop_Run advances once per step whether the extraction launch has no
+    receivers (one block, index advance only) or several blocks of them (the last block to finish
+    advances it): the run equals TimeStep + WFD_Inject (+ WFD_Extract) per step, bitwise."""
+    import torch
+    from tests.harness import ABIRunner, make_model
+    name, shape = "Prop2DAcoIsoDenQ_DEO2_FDTD", (44, 1, 38)
+    nz, ny, nx = shape
+    nt, nsteps = 40, 13
+    runs = []
+    for mode in ("run", "steps"):
+        g = ABIRunner(lib, name, shape, fs=True)
+        lib.WFD_Prop_SetStrict(ctypes.c_void_p(g.p), 1)
+        g.load(make_model(2, "iso", shape, seed=6))
+        ncell = nz * ny * nx
+        src = (SourcePoint32 * 1)(SourcePoint32(ncell // 2 + 5, 1, 1.0))
+        ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), 1, 0)
+        tr = None
+        if nrec:
+            rec = (SourcePoint32 * nrec)(*[SourcePoint32((7 * i) % ncell, i + 1, 1.0) for i in range(nrec)])
+            tr = lib.WFD_Points_Create(ctypes.cast(rec, ctypes.POINTER(SourcePoint32)), nrec, 1)
+        wav = torch.from_numpy(np.random.default_rng(2).standard_normal(nt).astype(np.float32)).cuda()
+        trc = torch.zeros(max(nrec, 1) * nt, device="cuda")
+        torch.cuda.synchronize()
+        stream = ctypes.c_void_p(lib.WFD_Prop_Stream(ctypes.c_void_p(g.p)))
+        if mode == "run":
+            assert lib.WFD_Prop_Run(ctypes.c_void_p(g.p), nsteps, 1, ts, ctypes.c_void_p(wav.data_ptr()), tr,
+                                    ctypes.c_void_p(trc.data_ptr()) if nrec else None, nt, 1) == 0
+        else:
+            for it in range(1, 1 + nsteps):
+                assert lib.WFD_Prop_TimeStepAsync(ctypes.c_void_p(g.p), 1, 0) == 0
+                pc = ctypes.c_void_p(ctypes.cast(g.abi.getPCur(g.p), ctypes.c_void_p).value)
+                assert lib.WFD_Inject(ts, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, stream) == 0
+                if nrec:
+                    assert lib.WFD_Extract(tr, ctypes.c_void_p(trc.data_ptr()), pc, it, nt, stream) == 0
+        assert lib.WFD_Prop_Synchronize(ctypes.c_void_p(g.p)) == 0
+        runs.append(({k: g.arr(k).copy() for k in ("PCur", "POld", "PSpace")}, trc.cpu().numpy()))
+        lib.WFD_Points_Free(ts)
+        if tr:
+            lib.WFD_Points_Free(tr)
+        g.close()
+    (fa, ta), (fb, tb) = runs
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), (k, mismatch_report(fa[k], fb[k]))
+    assert np.array_equal(ta, tb)
+    if nrec:
+        assert np.count_nonzero(ta.reshape(nrec, nt)[:, :nsteps]) > 0
+
+
 @pytest.mark.parametrize("name,shape", [("Prop3DAcoIsoDenQ_DEO2_FDTD", (36, 21, 30)),
                                         ("Prop3DAcoIsoDenQ_DEO2_FDTD", (37, 21, 30)),
                                         ("Prop3DAcoVTIDenQ_DEO2_FDTD", (28, 22, 24)),
