@@ -677,8 +677,9 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
                      "kernel": "whole step (kernels of " + W["name"] + " + injection + extraction)",
                      "algorithmic_bytes_per_cell": W["bytes_per_cell"], "kernel_ms": round(ms / K, 5),
                      "peak_source": peak_src},
-        # per step: the step kernel(s), the injection, the extraction with the time-index advance
-        "gpu_launches": K * (lib.WFD_Prop_StepKernels(prop.p) + 2),
+        # per step: the step kernel(s), the injection unless the step kernel applied it, the extraction
+        # with the time-index advance (WFD_Prop_StepKernels after WFD_Prop_Run)
+        "gpu_launches": K * lib.WFD_Prop_StepKernels(prop.p),
         "clocks": clk.summary(),
     }
     del traces, wav, d_wav, d_trc, h_trc, h_wav

@@ -300,7 +300,9 @@ int WFD_Prop_Prefetch(void *p);
 /* the object's CUDA stream (a cudaStream_t) */
 void *WFD_Prop_Stream(void *p);
 /* kernels the last time step launched: 1 = fused single-sweep kernel, 2 = the two passes (one more
- * when a source illumination sum is attached and the step kernel does not accumulate it itself) */
+ * when a source illumination sum is attached and the step kernel does not accumulate it itself);
+ * after WFD_Prop_Run, the launches per step of its loop (step kernels, the injection unless the step
+ * kernel applied it, the extraction) */
 int WFD_Prop_StepKernels(void *p);
 /* Source illumination fused into the time step: with a device sum attached (ncells floats), every
  * later step adds pCur^2 (the field the step reads) to it, as illum_accumulate_float would; the 3D

@@ -6,11 +6,14 @@ using namespace wfd;
 
 int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
     Fields Fn = F;
-    Fn.illum = nullptr;  // only the TMA-staged Iso kernel accumulates the illumination itself
+    Fn.illum = nullptr;    // only the TMA-staged Iso kernel accumulates the illumination itself
+    Fn.inj.ngroups = 0;    // and only the 2D Iso kernel applies a source injection itself
     if (g.ndim == 3 && phys == ISO) {
         // TMA-staged kernel when the tensor maps can be encoded (nz*4 a multiple of 16 bytes),
         // else the variant that stages its tiles with ordinary loads
-        if (fused_iso3d_tma(g, F, s)) return F.illum ? 2 : 1;
+        Fields Fi = F;
+        Fi.inj.ngroups = 0;
+        if (fused_iso3d_tma(g, Fi, s)) return 1 | (F.illum ? 2 : 0);
         return fused_iso3d(g, Fn, s) ? 1 : 0;
     }
     if (g.ndim == 3 && phys == VTI) {
@@ -19,7 +22,11 @@ int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_
         return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
     }
     if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
-    if (g.ndim == 2 && phys == ISO) return fused_iso2d(g, Fn, s) ? 1 : 0;
+    if (g.ndim == 2 && phys == ISO) {
+        Fields Fi = Fn;
+        Fi.inj = F.inj;
+        return fused_iso2d(g, Fi, s) ? 1 | (F.inj.ngroups ? 4 : 0) : 0;
+    }
     return 0;
 }
 

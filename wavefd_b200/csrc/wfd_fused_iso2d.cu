@@ -11,7 +11,8 @@
 // the update to its cells. Free surface: pCur above kz = 0 is its antisymmetric image (D+ input),
 // the z output above kz = 0 its symmetric image (D- input), as in propagatorStaticFunctions.h.
 // Cell arithmetic is the expression trees of the two-pass kernels (wfd_generic.cu), so the strict
-// build gives their bits.
+// build gives their bits. In a graph-replayed time loop the kernel also applies the step's source
+// injection to the cells of its tile (F.inj), which saves the injection launch.
 #include "wfd_kernels.h"
 
 namespace WFD_NS {
@@ -151,6 +152,25 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
             const float pc = F.pcur[k], po = F.pold[k];
             F.pold[k] = dt2V2_B * L - F.q[k] * (pc - po) - po + 2 * pc;
             F.pspace[k] = L;
+        }
+    }
+
+    // source injection into the new field (graph-replayed loops): the groups whose cell lies in this
+    // tile, after the tile's cells are written (visible to the CTA after the barrier); each group's
+    // contributions in order, separate IEEE multiply and add, as the injection kernel does
+    if (F.inj.ngroups) {
+        const long it = *F.inj.d_it;
+        if (it >= 1 && it <= F.inj.nt) {
+            __syncthreads();
+            for (long gi = threadIdx.x; gi < F.inj.ngroups; gi += NT) {
+                const long key = F.inj.key[gi];
+                const long x = key / nz, z = key - x * nz;
+                if (x < x0 || x >= x0 + TX || z < z0 || z >= z0 + TZ) continue;
+                float acc = F.pold[key];
+                for (long j = F.inj.start[gi]; j < F.inj.start[gi + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(F.inj.c[j], F.inj.wav[F.inj.other[j] * F.inj.nt + (it - 1)]));
+                F.pold[key] = acc;
+            }
         }
     }
 }

@@ -11,10 +11,23 @@
 namespace wfd {
 
 // Model and wavefield arrays of one propagator object (device-accessible pointers).
+// A source injection that a step kernel applies to the field it writes (graph-replayed time loops,
+// where the time index sits in device memory): new field[key[g]] += c[j] * wav[other[j] * nt + it-1]
+// for j = start[g] .. start[g+1]-1 in order, each product and sum rounded (IEEE), it = *d_it,
+// nothing when it is outside 1..nt. ngroups = 0: no injection in the step kernel.
+struct StepInject {
+    long ngroups;
+    const long *key, *start, *other;
+    const float *c, *wav;
+    long nt;
+    const long *d_it;
+};
+
 struct Fields {
     float *v, *b, *q, *eps, *eta, *f, *st, *ct, *sp, *cp;
     float *pcur, *pold, *pspace, *mcur, *mold, *mspace;
     float *illum;  // source illumination sum (sum over steps of pCur^2), or nullptr
+    StepInject inj;
 };
 
 // Scratch of the unfused passes (the reference's tmp arrays), device memory.
@@ -59,8 +72,8 @@ struct TileInfo {
     void pass1(const wfd::Grid &g, int phys, const wfd::Fields &F, const wfd::Scratch &S, cudaStream_t s); \
     void pass2(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, const wfd::Scratch &S,    \
                cudaStream_t s);                                                                          \
-    /* fused single-sweep steps; 0 when the geometry is not handled, 1 when stepped, 2 when stepped  \
-       with F.illum accumulated inside the step kernel */                                               \
+    /* fused single-sweep steps; 0 when the geometry is not handled, else flags: 1 stepped, 2 F.illum \
+       accumulated inside the step kernel, 4 F.inj applied inside the step kernel */                    \
     int fused_step(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);      \
     void scale(const wfd::Grid &g, const wfd::Fields &F, bool two, cudaStream_t s);                      \
     void dplus(const wfd::Grid &g, const float *in, float *ox, float *oy, float *oz, cudaStream_t s);    \

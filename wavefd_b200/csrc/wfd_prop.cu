@@ -98,6 +98,7 @@ Fields Prop::fields() const {
     F.mold = field[F_MOLD];
     F.mspace = field[F_MSPACE];
     F.illum = illum;
+    F.inj = inj;
     return F;
 }
 
@@ -280,11 +281,13 @@ int prop_step(Prop *p, bool linear, bool sync) {
     Grid g = p->grid();
     Fields F = p->fields();
     bool done = false, illum_done = false;
+    p->inject_done = false;
     if (p->fused) {
         const int r = p->strict ? wfd_strict::fused_step(g, p->phys, linear, F, p->stream)
                                 : wfd_fast::fused_step(g, p->phys, linear, F, p->stream);
-        done = r > 0;
-        illum_done = r == 2;
+        done = (r & 1) != 0;
+        illum_done = (r & 2) != 0;
+        p->inject_done = (r & 4) != 0;
     }
     if (!done) {
         if (!ensure_scratch(p, p->phys == ISO ? 3 : 6)) return p->status;

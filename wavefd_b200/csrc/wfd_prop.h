@@ -39,6 +39,8 @@ struct Prop {
     std::string message;
     long steps = 0;
     int step_kernels = 0;  // kernels launched by the last time step (1 fused, 2 unfused)
+    StepInject inj{};      // a source injection for the step kernel to apply (WFD_Prop_Run), or none
+    bool inject_done = false;  // the last step kernel applied `inj`
 
     long ncells() const { return nx * ny * nz; }
     Grid grid() const;

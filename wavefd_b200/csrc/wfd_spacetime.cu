@@ -318,7 +318,9 @@ int run_step(Prop *p, DeviceTable *src, const float *wav, DeviceTable *rec, floa
     if (int rc = wfd::prop_step(p, false, false)) return rc;
     float *pc = p->field[wfd::F_PCUR];
     cudaStream_t s = p->stream;
-    if (src && src->t.ngroups)
+    const bool inject = src && src->t.ngroups && !p->inject_done;  // unless the step kernel did it
+    p->step_kernels += (inject ? 1 : 0) + 1;  // launches per step of the loop
+    if (inject)
         wfd::k_scatter_groups_devit<<<wfd::nb(src->t.ngroups), 256, 0, s>>>(
             src->t.ngroups, src->t.d_key, src->t.d_start, src->t.d_other, src->t.d_c, 0, pc, const_cast<float *>(wav),
             nt, d_it);
@@ -353,6 +355,12 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     const long init[2] = {it0, 0};
     cudaMemcpyAsync(d_it, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
+    // a step kernel that can apply the injection itself (the 2D Iso kernel) gets the source table;
+    // the per-CTA scan of the groups stays cheap for tables of up to 1024 groups
+    p->inj = wfd::StepInject{};
+    if (src && src->t.ngroups && src->t.ngroups <= 1024)
+        p->inj = wfd::StepInject{src->t.ngroups, src->t.d_key, src->t.d_start, src->t.d_other, src->t.d_c,
+                                 wavelet, nt, d_it};
     long done = 0;
     int rc = WFD_OK;
     if (use_graph && nsteps >= 2) {
@@ -382,6 +390,7 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
         }
     }
     for (; !rc && done < nsteps; done++) rc = run_step(p, src, wavelet, rec, traces, nt, d_it);
+    p->inj = wfd::StepInject{};
     cudaFreeAsync(d_it, s);
     return rc;
 }
