@@ -105,6 +105,24 @@ __device__ __forceinline__ float2 st8z(const Grid &g, const float (&v)[10], int 
     auto w = [&](int i) { return make_float2(v[o + i], v[o + i + 1]); };
     return st8(g, w(0), w(1), w(2), w(3), w(4), w(5), w(6), w(7));
 }
+// A derivative: the inverse spacing `id` times the stencil. The strict build multiplies the stencil
+// sum (the reference's order); the fast build folds `id` into the four coefficients (one multiply
+// fewer per derivative).
+__device__ __forceinline__ float2 st8d(const Grid &g, float id, float2 w0, float2 w1, float2 w2, float2 w3, float2 w4,
+                                       float2 w5, float2 w6, float2 w7) {
+#if WFD_STRICT
+    return mul2(bc2(id), st8(g, w0, w1, w2, w3, w4, w5, w6, w7));
+#else
+    float2 s = mul2(bc2(g.c1 * id), sub2(w4, w3));
+    s = fma2(bc2(g.c2 * id), sub2(w5, w2), s);
+    s = fma2(bc2(g.c3 * id), sub2(w6, w1), s);
+    return fma2(bc2(g.c4 * id), sub2(w7, w0), s);
+#endif
+}
+__device__ __forceinline__ float2 st8zd(const Grid &g, float id, const float (&v)[10], int o) {
+    auto w = [&](int i) { return make_float2(v[o + i], v[o + i + 1]); };
+    return st8d(g, id, w(0), w(1), w(2), w(3), w(4), w(5), w(6), w(7));
+}
 __device__ __forceinline__ void load10(float (&v)[10], const float *p) {
 #pragma unroll
     for (int i = 0; i < 5; i++) {
@@ -136,26 +154,26 @@ __device__ __forceinline__ Out6 pass1(const Grid &g, const float *const (&ring)[
     const float2 zero = bc2(0.0f);
     float2 dPx = zero, dPy = zero, dPz = zero, dMx = zero, dMy = zero, dMz = zero;
     if (need_x) {
-        dPx = mul2(bc2(g.idx), st8(g, ld2(ring[0] + off), ld2(ring[1] + off), ld2(ring[2] + off), ld2(ring[3] + off),
-                                   ld2(ring[4] + off), ld2(ring[5] + off), ld2(ring[6] + off), ld2(ring[7] + off)));
+        dPx = st8d(g, g.idx, ld2(ring[0] + off), ld2(ring[1] + off), ld2(ring[2] + off), ld2(ring[3] + off),
+                   ld2(ring[4] + off), ld2(ring[5] + off), ld2(ring[6] + off), ld2(ring[7] + off));
         const int o = off + RBOX;
-        dMx = mul2(bc2(g.idx), st8(g, ld2(ring[0] + o), ld2(ring[1] + o), ld2(ring[2] + o), ld2(ring[3] + o),
-                                   ld2(ring[4] + o), ld2(ring[5] + o), ld2(ring[6] + o), ld2(ring[7] + o)));
+        dMx = st8d(g, g.idx, ld2(ring[0] + o), ld2(ring[1] + o), ld2(ring[2] + o), ld2(ring[3] + o),
+                   ld2(ring[4] + o), ld2(ring[5] + o), ld2(ring[6] + o), ld2(ring[7] + o));
     }
     if (need_y) {
         const float *p = cp;
-        dPy = mul2(bc2(g.idy), st8(g, ld2(p - 3 * RZW), ld2(p - 2 * RZW), ld2(p - RZW), ld2(p), ld2(p + RZW),
-                                   ld2(p + 2 * RZW), ld2(p + 3 * RZW), ld2(p + 4 * RZW)));
+        dPy = st8d(g, g.idy, ld2(p - 3 * RZW), ld2(p - 2 * RZW), ld2(p - RZW), ld2(p), ld2(p + RZW),
+                   ld2(p + 2 * RZW), ld2(p + 3 * RZW), ld2(p + 4 * RZW));
         p = cp + RBOX;
-        dMy = mul2(bc2(g.idy), st8(g, ld2(p - 3 * RZW), ld2(p - 2 * RZW), ld2(p - RZW), ld2(p), ld2(p + RZW),
-                                   ld2(p + 2 * RZW), ld2(p + 3 * RZW), ld2(p + 4 * RZW)));
+        dMy = st8d(g, g.idy, ld2(p - 3 * RZW), ld2(p - 2 * RZW), ld2(p - RZW), ld2(p), ld2(p + RZW),
+                   ld2(p + 2 * RZW), ld2(p + 3 * RZW), ld2(p + 4 * RZW));
     }
     if (need_z) {
         float v[10];
         load10(v, cp - 4);
-        dPz = mul2(bc2(g.idz), st8z(g, v, 1));
+        dPz = st8zd(g, g.idz, v, 1);
         load10(v, cp + RBOX - 4);
-        dMz = mul2(bc2(g.idz), st8z(g, v, 1));
+        dMz = st8zd(g, g.idz, v, 1);
     }
     if (zero_xy) {  // free-surface row kz = 0 (lane x): the x and y derivatives are zero
         dPx.x = 0.0f;
@@ -239,8 +257,8 @@ __device__ __forceinline__ void queue_phase(const Grid &g, float2 (&qx)[8][2], f
     qx[N][1] = c.mx;
 #pragma unroll
     for (int f = 0; f < 2; f++)
-        sx[f] = st8(g, qx[(PH + 4) & 7][f], qx[(PH + 5) & 7][f], qx[(PH + 6) & 7][f], qx[(PH + 7) & 7][f],
-                    qx[(PH + 0) & 7][f], qx[(PH + 1) & 7][f], qx[(PH + 2) & 7][f], qx[N][f]);
+        sx[f] = st8d(g, g.idx, qx[(PH + 4) & 7][f], qx[(PH + 5) & 7][f], qx[(PH + 6) & 7][f], qx[(PH + 7) & 7][f],
+                     qx[(PH + 0) & 7][f], qx[(PH + 1) & 7][f], qx[(PH + 2) & 7][f], qx[N][f]);
     qc[N4][0] = c.py;
     qc[N4][1] = c.pz;
     qc[N4][2] = c.my;
@@ -524,12 +542,12 @@ __global__ void __launch_bounds__(NT, 1)
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
                     const float *ty = TYs + f * TYR * TZ + row * TZ + 2 * zp;
-                    const float2 sy = st8(g, ld2(ty), ld2(ty + TZ), ld2(ty + 2 * TZ), ld2(ty + 3 * TZ),
-                                          ld2(ty + 4 * TZ), ld2(ty + 5 * TZ), ld2(ty + 6 * TZ), ld2(ty + 7 * TZ));
+                    const float2 dy = st8d(g, g.idy, ld2(ty), ld2(ty + TZ), ld2(ty + 2 * TZ), ld2(ty + 3 * TZ),
+                                           ld2(ty + 4 * TZ), ld2(ty + 5 * TZ), ld2(ty + 6 * TZ), ld2(ty + 7 * TZ));
                     float v[10];
                     load10(v, TZs + f * TY * TZW + row * TZW + 2 * zp);
-                    const float2 sz = st8z(g, v, 0);
-                    L[f] = fma2(bc2(g.idz), sz, fma2(bc2(g.idy), sy, mul2(bc2(g.idx), sx[f])));
+                    const float2 dz = st8zd(g, g.idz, v, 0);
+                    L[f] = add2(add2(sx[f], dy), dz);  // dx + dy + dz (sx[f] is dx)
                 }
                 const bool ok = j >= 4 && j < g.nx - 4 && yz_tile;
                 if (top && zp == 0) {  // free-surface row: every derivative is zero
