@@ -99,12 +99,6 @@ __device__ __forceinline__ float2 st8(const Grid &g, float2 w0, float2 w1, float
     s = fma2(bc2(g.c3), sub2(w6, w1), s);
     return fma2(bc2(g.c4), sub2(w7, w0), s);
 }
-// stencil along z of a cell pair from ten consecutive values v[0..9]: lane x takes v[o..o+7],
-// lane y v[o+1..o+8]
-__device__ __forceinline__ float2 st8z(const Grid &g, const float (&v)[10], int o) {
-    auto w = [&](int i) { return make_float2(v[o + i], v[o + i + 1]); };
-    return st8(g, w(0), w(1), w(2), w(3), w(4), w(5), w(6), w(7));
-}
 // A derivative: the inverse spacing `id` times the stencil. The strict build multiplies the stencil
 // sum (the reference's order); the fast build folds `id` into the four coefficients (one multiply
 // fewer per derivative).
@@ -119,6 +113,8 @@ __device__ __forceinline__ float2 st8d(const Grid &g, float id, float2 w0, float
     return fma2(bc2(g.c4 * id), sub2(w7, w0), s);
 #endif
 }
+// the same along z for a cell pair from ten consecutive values v[0..9]: lane x takes v[o..o+7],
+// lane y v[o+1..o+8]
 __device__ __forceinline__ float2 st8zd(const Grid &g, float id, const float (&v)[10], int o) {
     auto w = [&](int i) { return make_float2(v[o + i], v[o + i + 1]); };
     return st8d(g, id, w(0), w(1), w(2), w(3), w(4), w(5), w(6), w(7));
