@@ -306,7 +306,8 @@ void *WFD_Prop_Stream(void *p);
 int WFD_Prop_StepKernels(void *p);
 /* Source illumination fused into the time step: with a device sum attached (ncells floats), every
  * later step adds pCur^2 (the field the step reads) to it, as illum_accumulate_float would; the 3D
- * Iso step kernel does it in place of a separate pass. NULL detaches. */
+ * Iso, VTI and TTI step kernels (nz a multiple of 4) do it in place of a separate pass. NULL
+ * detaches. */
 int WFD_Prop_SetIllumination(void *p, float *accum);
 /* nsteps time steps of the object (TimeStep, then injection into pCur at time index it, then
  * extraction of pCur at it, it = it0, it0+1, ...; either table may be NULL), with every pair of steps

@@ -313,10 +313,13 @@ def test_prop_run_index_advance(lib, nrec):
 @pytest.mark.parametrize("name,shape", [("Prop3DAcoIsoDenQ_DEO2_FDTD", (36, 21, 30)),
                                         ("Prop3DAcoIsoDenQ_DEO2_FDTD", (37, 21, 30)),
                                         ("Prop3DAcoVTIDenQ_DEO2_FDTD", (28, 22, 24)),
+                                        ("Prop3DAcoVTIDenQ_DEO2_FDTD", (30, 22, 24)),
+                                        ("Prop3DAcoTTIDenQ_DEO2_FDTD", (28, 22, 24)),
                                         ("Prop2DAcoIsoDenQ_DEO2_FDTD", (44, 1, 38))])
 def test_illumination_fused_into_step(lib, name, shape):
-    """WFD_Prop_SetIllumination: every step adds pCur^2 (the field it reads) to the sum, inside the 3D Iso
-    step kernel (nz % 4 == 0) or as a separate pass otherwise; bitwise against float32 numpy."""
+    """WFD_Prop_SetIllumination: every step adds pCur^2 (the field it reads) to the sum, inside the 3D
+    Iso, VTI and TTI step kernels (nz % 4 == 0) or as a separate pass otherwise (nz % 4 != 0, 2D);
+    bitwise against float32 numpy."""
     import torch
     from tests.harness import ABIRunner, make_model
     from wavefd_b200.abi import PROPAGATORS

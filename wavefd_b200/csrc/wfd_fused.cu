@@ -6,8 +6,11 @@ using namespace wfd;
 
 int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
     Fields Fn = F;
-    Fn.illum = nullptr;    // only the TMA-staged Iso kernel accumulates the illumination itself
-    Fn.inj.ngroups = 0;    // and only the 2D Iso kernel applies a source injection itself
+    Fn.illum = nullptr;    // the TMA-staged Iso, VTI and TTI kernels accumulate the illumination
+    Fn.inj.ngroups = 0;    // themselves; only the 2D Iso kernel applies a source injection itself
+    Fields Fl = Fn;
+    Fl.illum = F.illum;
+    const int lit = F.illum ? 2 : 0;
     if (g.ndim == 3 && phys == ISO) {
         // TMA-staged kernel when the tensor maps can be encoded (nz*4 a multiple of 16 bytes),
         // else the variant that stages its tiles with ordinary loads
@@ -18,10 +21,10 @@ int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_
     }
     if (g.ndim == 3 && phys == VTI) {
         // the VTI kernel with x-direction register queues, else the ring-staged kernel TTI uses
-        if (fused_vti3d_tma(g, linear, Fn, s)) return 1;
+        if (fused_vti3d_tma(g, linear, Fl, s)) return 1 | lit;
         return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
     }
-    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
+    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fl, s) ? 1 | lit : 0;
     if (g.ndim == 2 && phys == ISO) {
         Fields Fi = Fn;
         Fi.inj = F.inj;

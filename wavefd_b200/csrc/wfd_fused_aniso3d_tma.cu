@@ -22,8 +22,9 @@
 // Region rules (interior [4,n-4), free-surface rows, untouched annulus) are selects. The free
 // surface images are written into shared memory: the antisymmetric image of pCur/mCur above
 // kz = 0 into each ring plane of the top tile, the symmetric image of the z outputs into the halo
-// columns of the top tile. Waits are bounded; on timeout the kernel records an error in a device
-// status word and leaves. Requires nz % 4 == 0 (TMA row pitch).
+// columns of the top tile. With an illumination sum attached (single objects), each cell's pCur^2
+// is added to it as the cell is updated. Waits are bounded; on timeout the kernel records an error
+// in a device status word and leaves. Requires nz % 4 == 0 (TMA row pitch).
 #include "wfd_kernels.h"
 #include "wfd_tma.cuh"
 
@@ -562,6 +563,15 @@ __global__ void __launch_bounds__(NT, 1)
                     const float2 np = add2(t, mul2(bc2(2.0f), pc));
                     st2((f == 0 ? out_pold : out_mold) + k, ok ? np : po);
                     if (!LINEAR) st2((f == 0 ? out_pspace : out_mspace) + k, ok ? L[f] : bc2(0.0f));
+                }
+                if (!BATCH && F.illum) {
+                    // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add,
+                    // as illumination.c:31-53 does)
+                    const float2 pcp = ld2(ring[0] + ro);
+                    float2 a = ld2(F.illum + k);
+                    a.x = __fadd_rn(a.x, __fmul_rn(pcp.x, pcp.x));
+                    a.y = __fadd_rn(a.y, __fmul_rn(pcp.y, pcp.y));
+                    st2(F.illum + k, a);
                 }
             }
             __syncthreads();

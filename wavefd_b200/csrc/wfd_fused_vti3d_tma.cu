@@ -21,7 +21,9 @@
 // images (antisymmetric pCur/mCur above kz = 0 in the z derivative, symmetric z outputs in D-) only
 // in the top tile. Persistent CTAs loop over (tile, x-chunk) items; chunks start with 14 warm-up
 // planes that only fill the queues (their groups load the queue boxes alone). Waits are bounded;
-// on timeout the kernel records an error in a device status word and leaves. Requires nz % 4 == 0.
+// on timeout the kernel records an error in a device status word and leaves. With an illumination
+// sum attached (single objects), each cell's pCur^2 is added to it as the cell is updated.
+// Requires nz % 4 == 0.
 #include "wfd_kernels.h"
 #include "wfd_tma.cuh"
 
@@ -464,6 +466,14 @@ __global__ void __launch_bounds__(NT, 2)
                         st2((f == 0 ? o_po : o_mo) + k, make_float2(ok0 ? np.x : po.x, ok1 ? np.y : po.y));
                         if (!LINEAR)
                             st2((f == 0 ? o_ps : o_ms) + k, make_float2(ok0 ? L[f].x : 0.0f, ok1 ? L[f].y : 0.0f));
+                    }
+                    if (!BATCH && F.illum) {
+                        // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and
+                        // add, as illumination.c:31-53 does)
+                        float2 a = ld2(F.illum + k);
+                        a.x = __fadd_rn(a.x, __fmul_rn(pc[0].x, pc[0].x));
+                        a.y = __fadd_rn(a.y, __fmul_rn(pc[0].y, pc[0].y));
+                        st2(F.illum + k, a);
                     }
                 }
             }
