@@ -91,6 +91,7 @@ __device__ __forceinline__ float2 sel2(bool c, float2 a, float2 b) { return c ? 
 __device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
 __device__ __forceinline__ float2 div2(float2 a, float2 b) { return make_float2(a.x / b.x, a.y / b.y); }
 
+#if WFD_STRICT
 // 8-point staggered stencil c1(w4-w3) + c2(w5-w2) + c3(w6-w1) + c4(w7-w0), summed left to right:
 // D+ with w = f(k-3..k+4), D- with w = f(k-4..k+3) (prop3DAcoIsoDenQ_DEO2_FDTD.h:846-864, :1113-1131)
 __device__ __forceinline__ float2 st8(const Grid &g, float2 w0, float2 w1, float2 w2, float2 w3, float2 w4,
@@ -100,6 +101,7 @@ __device__ __forceinline__ float2 st8(const Grid &g, float2 w0, float2 w1, float
     s = fma2(bc2(g.c3), sub2(w6, w1), s);
     return fma2(bc2(g.c4), sub2(w7, w0), s);
 }
+#endif
 // A derivative: the inverse spacing `id` times the stencil. The strict build multiplies the stencil
 // sum (the reference's order); the fast build folds `id` into the four coefficients (one multiply
 // fewer per derivative).

@@ -82,9 +82,8 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float mul1(float a, float b) { return a * b; }
 __device__ __forceinline__ float add1(float a, float b) { return a + b; }
-// Negation and subtraction as one packed instruction each: b * -1 is exact, so b * -1 + a rounds
-// once, like -b + a (a negated operand of the packed add would cost two scalar instructions).
-__device__ __forceinline__ float2 neg2(float2 a) { return __fmul2_rn(a, make_float2(-1.0f, -1.0f)); }
+// Subtraction as one packed instruction: b * -1 is exact, so b * -1 + a rounds once, like -b + a (a
+// negated operand of the packed add would cost two scalar instructions).
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 #endif
 __device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
