@@ -84,6 +84,34 @@ void wfo_interpforward_double(const double *h, double *d, const double *m, long 
 /* illumination.c:3-53 (float): field = field^2 when accum is NULL, else accum += field^2 */
 void wfo_illum_float(float *accum, float *field, long n);
 
+/* FP64 rerun: the time steps, scaling, standalone D+/D-, Born injection and imaging conditions
+ * (V, VB, B for Iso; V for VTI/TTI) and injection/extraction above, evaluated in double precision
+ * on double arrays (wfo_generic.inc instantiated with double). */
+void wfo64_step_iso(const wfo_geom *g, const double *v, const double *b, const double *q,
+                    const double *pcur, double *pold, double *pspace);
+void wfo64_step_vti(const wfo_geom *g, long linear, const double *v, const double *eps, const double *eta,
+                    const double *b, const double *f, const double *q, const double *pcur,
+                    const double *mcur, double *pold, double *mold, double *pspace, double *mspace);
+void wfo64_step_tti(const wfo_geom *g, const double *v, const double *eps, const double *eta,
+                    const double *b, const double *f, const double *q, const double *sint,
+                    const double *cost, const double *sinp, const double *cosp, const double *pcur,
+                    const double *mcur, double *pold, double *mold, double *pspace, double *mspace);
+void wfo64_scale(const wfo_geom *g, const double *v, const double *b, double *pspace, double *mspace);
+void wfo64_dplus(const wfo_geom *g, const double *in, double *outx, double *outy, double *outz);
+void wfo64_dminus(const wfo_geom *g, const double *in, double *outx, double *outy, double *outz);
+void wfo64_born_iso(const wfo_geom *g, long which, const double *v, const double *b, const double *dv,
+                    const double *db, const double *p, const double *dp, double *pcur);
+void wfo64_born_aniso_v(const wfo_geom *g, const double *v, const double *dv, const double *dp,
+                        const double *dm, double *pcur, double *mcur);
+void wfo64_image_iso(const wfo_geom *g, long which, const double *v, const double *b, const double *p,
+                     const double *dp, const double *pold, double *dv, double *db);
+void wfo64_image_aniso_v(const wfo_geom *g, const double *v, const double *b, const double *dp,
+                         const double *dm, const double *pold, const double *mold, double *dv);
+void wfo64_inject(double *field, const double *data, long it, long nt, const long *iu, const long *ir,
+                  const double *c, long n);
+void wfo64_extract(double *data, const double *field, long it, long nt, const long *iu, const long *ir,
+                   const double *c, long n);
+
 #ifdef __cplusplus
 }
 #endif

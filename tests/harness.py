@@ -134,6 +134,51 @@ class OracleRunner:
         self.o.scale(self.g, a["V"], a["B"], a["PSpace"], None if self.physics == "iso" else a["MSpace"])
 
 
+class OracleRunner64:
+    """The FP64 rerun of the restatement with the same object semantics: the FP32 model (Q from the
+    FP32 profile) promoted to double, then every step in double precision."""
+
+    def __init__(self, oracle, name, shape, fs=True, nsponge=6, dx=0.01, dt=0.001, freqQ=5.0, qMin=0.1,
+                 qInterior=100.0):
+        base = OracleRunner(oracle, name, shape, fs=fs, nsponge=nsponge, dx=dx, dt=dt, freqQ=freqQ, qMin=qMin,
+                            qInterior=qInterior)
+        self.o, self.g, self.physics, self.ndim = oracle, base.g, base.physics, base.ndim
+        self.a = {k: v.astype(np.float64) for k, v in base.a.items()}
+
+    def load(self, model):
+        for k, v in model.items():
+            self.a[k][...] = v
+
+    def arr(self, k):
+        return self.a[k]
+
+    def step(self, linear=False):
+        a, o, g = self.a, self.o, self.g
+        if self.physics == "iso":
+            o.step_iso64(g, a["V"], a["B"], a["DtOmegaInvQ"], a["PCur"], a["POld"], a["PSpace"])
+        elif self.physics == "vti":
+            o.step_vti64(g, linear, a["V"], a["Eps"], a["Eta"], a["B"], a["F"], a["DtOmegaInvQ"], a["PCur"],
+                         a["MCur"], a["POld"], a["MOld"], a["PSpace"], a["MSpace"])
+        else:
+            o.step_tti64(g, a["V"], a["Eps"], a["Eta"], a["B"], a["F"], a["DtOmegaInvQ"], a["SinTheta"],
+                         a["CosTheta"], a["SinPhi"], a["CosPhi"], a["PCur"], a["MCur"], a["POld"], a["MOld"],
+                         a["PSpace"], a["MSpace"])
+        a["PCur"], a["POld"] = a["POld"], a["PCur"]
+        a["MCur"], a["MOld"] = a["MOld"], a["MCur"]
+
+
+class Ref64Runner(OracleRunner64):
+    """The reference's own passes instantiated with double (oracle Ref64), same object semantics."""
+
+    def __init__(self, ref64, oracle, name, shape, **kw):
+        super().__init__(oracle, name, shape, **kw)
+        self.r = ref64
+        self.scratch = ref64.new_scratch(self.a["V"].shape)
+
+    def step(self, linear=False):
+        self.r.step(self.physics, self.ndim, self.g, self.a, self.scratch, linear=linear)
+
+
 def same(a, b):
     """Bitwise equality up to the sign of zero."""
     return np.array_equal(a, b)
