@@ -64,3 +64,54 @@ def test_header_covers_reference_exports(libpath):
         ref = {s for s in ref if s.startswith("Prop") or s.endswith("data_float") or s.endswith("data_double")}
         assert ref <= ours, (f, sorted(ref - ours))
         assert ref <= decl, (f, sorted(ref - decl))
+
+
+# ---- signatures: the header's Part 1 prototypes against the reference's own definitions ----------
+REF_SRC = os.environ.get("WAVEFD_REFERENCE_SRC") or os.path.join(os.path.dirname(ROOT), "reference", "src")
+
+
+def _norm_type(decl):
+    """ABI type of one parameter or return declaration: qualifiers that do not change the C ABI
+    (const, __restrict__) dropped, the parameter name dropped, pointers attached to the type."""
+    d = re.sub(r"\b(const|__restrict__|restrict)\b", " ", decl)
+    d = re.sub(r"\s*\*\s*", " * ", d).split()
+    if len(d) > 1 and re.match(r"^[A-Za-z_]\w*$", d[-1]) and d[-1] not in ("long", "float", "double", "int", "void",
+                                                                           "size_t", "char"):
+        d = d[:-1]  # parameter name
+    return " ".join(d).replace(" *", "*")
+
+
+def _prototypes(text, terminator):
+    """name -> (return type, [parameter types]) of every top-level C function declared (';') or
+    defined ('{') in text."""
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    out = {}
+    pat = re.compile(r"(?:^|[;}\n])\s*((?:[A-Za-z_][\w]*[\s\*]+)+?)([A-Za-z_]\w*)\s*\(([^()]*)\)\s*" +
+                     re.escape(terminator))
+    for m in pat.finditer(text):
+        ret, name, params = m.group(1), m.group(2), m.group(3)
+        if ret.strip() in ("return", "else") or "extern" in ret and '"C"' in ret:
+            continue
+        ret = ret.replace('extern "C"', "")
+        plist = [] if params.strip() in ("", "void") else [_norm_type(p) for p in params.split(",")]
+        out[name] = (_norm_type(ret + " x"), plist)
+    return out
+
+
+def test_header_signatures_match_reference_definitions():
+    if not os.path.isdir(REF_SRC):
+        pytest.skip("reference sources not present")
+    header = _prototypes(open(HEADER).read(), ";")
+    checked = 0
+    for f in sorted(os.listdir(REF_SRC)):
+        if not (f.startswith("prop") and f.endswith(".cc")) and f != "spacetime.cc":
+            continue
+        ref = _prototypes(open(os.path.join(REF_SRC, f)).read(), "{")
+        for name, sig in ref.items():
+            if not (name.startswith("Prop") or name.endswith("data_float") or name.endswith("data_double")):
+                continue
+            assert name in header, f"{f}: {name} not declared in the header"
+            assert header[name] == sig, f"{f}: {name}: header {header[name]} vs reference {sig}"
+            checked += 1
+    assert checked > 150, checked
