@@ -43,8 +43,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
-// Bounded wait for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, uint64_t limit_ns = 2000000000ull) {
+// Limit of the waits for tile loads (2 s), per translation unit. A test hook shortens it
+// (WFD_Debug_SetPipelineWait) so that a wait runs out while its copy is still in flight; the drain
+// waits at the end of a kernel pass their own limit and are not affected.
+static __device__ uint64_t d_pipeline_wait_ns = 2000000000ull;
+
+// Bounded wait for the phase with the given parity to complete; false on timeout. Without an
+// explicit limit the pipeline limit applies (read only once the first poll has failed).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, uint64_t limit_ns = 0) {
     const uint32_t addr = smem_u32(bar);
     uint32_t ok = 0;
     uint64_t t0 = 0;
@@ -57,8 +63,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, uint64
             : "r"(addr), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (spin == 0) t0 = globaltimer_ns();
-        else if (globaltimer_ns() - t0 > limit_ns) return false;
+        if (spin == 0) {
+            t0 = globaltimer_ns();
+            if (limit_ns == 0) limit_ns = *(volatile uint64_t *)&d_pipeline_wait_ns;
+        } else if (globaltimer_ns() - t0 > limit_ns) {
+            return false;
+        }
     }
 }
 
