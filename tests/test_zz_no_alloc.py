@@ -79,11 +79,45 @@ def test_no_alloc_matches_regular_entry_point(lib, name, nz, isfwi):
     gpu.close()
 
 
+@pytest.mark.parametrize("nz", [2047, 2048])  # the largest Bluestein length (fills the scratch) and the limit
+def test_no_alloc_at_the_size_limit(lib, nz):
+    """nz = 2047: n = 4094, Bluestein length 8192, 20478 of the scratch's 20480 entries; nz = 2048:
+    the largest accepted (power of two). Isotropic 2D, against the regular entry point."""
+    import torch
+    name = "Prop2DAcoIsoDenQ_DEO2_FDTD"
+    shape = (nz, 1, 12)
+    gpu = ABIRunner(lib, name, shape, fs=True)
+    gpu.load(make_model(2, "iso", shape, seed=3))
+    shp = gpu.arr("V").shape
+    rng = np.random.default_rng(5)
+    DP = (rng.standard_normal(shp) * 1e-2).astype(np.float32)
+    img0 = (rng.standard_normal(shp) * 1e-3).astype(np.float32)
+    ref = img0.copy()
+    for _ in range(2):
+        gpu.abi.AdjointBornAccumulation_wavefieldsep(gpu.p, fptr(ref), fptr(DP), 0)
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(gpu.p)) == 0
+    d_dp = torch.from_numpy(DP).cuda()
+    d_img = torch.from_numpy(img0).cuda()
+    ptr = lambda g: ctypes.c_void_p(ctypes.cast(getattr(gpu.abi, "get" + g)(gpu.p), ctypes.c_void_p).value)
+    for i in range(2):
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        rc = lib.WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(shp[0], 1, nz, 0, ptr("V"), ptr("B"), _dev(d_dp),
+                                                                  ptr("POld"), None, None, _dev(d_img), None)
+        assert rc == 0, lib.WFD_LastErrorMessage()
+        torch.cuda.synchronize()
+        if i == 1:  # the first call on a device may load the library's module; the second allocates nothing
+            assert torch.cuda.mem_get_info()[0] == free0, "device memory in use changed across a call"
+    err = rel_l2(d_img.cpu().numpy() - img0, ref - img0)
+    assert err <= TOL, f"nz={nz}: rel L2 of the accumulated term {err:.3e}"
+    gpu.close()
+
+
 def test_no_alloc_rejects_oversize_and_host_arrays(lib):
     import torch
     d = torch.zeros(16, device="cuda")
     p = _dev(d)
-    assert lib.WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(1, 1, 4096, 0, p, p, p, p, None, None, p, None) != 0
+    assert lib.WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(1, 1, 2049, 0, p, p, p, p, None, None, p, None) != 0
     h = np.zeros(64, np.float32)
     hp = ctypes.c_void_p(h.ctypes.data)
     assert lib.WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(2, 1, 32, 0, hp, hp, hp, hp, None, None, hp, None) != 0

@@ -6,9 +6,12 @@
 // (for example while other work holds the allocator), or plug-ins whose host application forbids
 // device allocations by extensions. The regular entry points allocate the Bluestein FFT tables and,
 // for host arrays, staging buffers on every call. This variant keeps its scratch (the tables) in a
-// fixed file-scope device array instead, builds them on the device each call, and requires every
-// array it is given to be device or managed memory.
+// fixed file-scope device array instead, builds them on the device when the FFT length differs from
+// the last call's on that device, and requires every array it is given to be device or managed
+// memory on the current device. The device address of the array is looked up once per device and
+// kept for the life of the process, so the entry point must not be used across a cudaDeviceReset.
 #include <math.h>
+#include <stdlib.h>
 
 #include <mutex>
 
@@ -28,6 +31,7 @@ static __device__ __align__(256) float2 g_sep_scratch[kScratch];
 
 std::mutex g_mu;
 float2 *g_addr[256];  // device address of g_sep_scratch, per device ordinal
+int g_tables_n[256];  // FFT length whose Bluestein tables the scratch of that device holds (0: none)
 
 // radix-2 FFT of length m (power of two) in shared memory, double precision:
 // a[k] <- sum_j a[j] e^{sign 2 pi i jk/m}
@@ -113,9 +117,22 @@ extern "C" int WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(long nx, long ny
             return fail("wavefieldsep_NoAlloc: every array must be device or managed memory");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return fail("wavefieldsep_NoAlloc: no device");
+    // the arrays must live on the current device: the scratch address below is this device's
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, dVel) != cudaSuccess ||
+        (attr.type == cudaMemoryTypeDevice && attr.device != dev))
+        return fail("wavefieldsep_NoAlloc: the image is not on the current device");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n = (int)(2 * nz);
+    int m = 0;
+    if (n & (n - 1)) {
+        m = 1;
+        while (m < 2 * n - 1) m <<= 1;
+    }
     float2 *scratch = nullptr;
     {
-        // set-up, once per device: the device address of the file-scope scratch array
+        // set-up, once per device, with that device current: the device address of the file-scope
+        // scratch array (the host name g_sep_scratch is not a device address)
         std::lock_guard<std::mutex> lk(g_mu);
         if (!g_addr[dev]) {
             void *p = nullptr;
@@ -125,18 +142,21 @@ extern "C" int WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(long nx, long ny
                 return WFD_ERR_CUDA;
             }
             g_addr[dev] = static_cast<float2 *>(p);
+            g_tables_n[dev] = 0;
         }
         scratch = g_addr[dev];
-    }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int n = (int)(2 * nz);
-    int m = 0;
-    if (n & (n - 1)) {
-        m = 1;
-        while (m < 2 * n - 1) m <<= 1;
-        const int smem = (int)(sizeof(double2) * (size_t)m);
-        cudaFuncSetAttribute(k_sep_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_sep_tables<<<1, 1024, smem, s>>>(n, m, scratch);
+        // the Bluestein tables depend on n only: rebuilt when the last call on this device had another n
+        if (m && g_tables_n[dev] != n) {
+            const int smem = (int)(sizeof(double2) * (size_t)m);
+            const cudaError_t e = cudaFuncSetAttribute(k_sep_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) {
+                wfd::set_global_error(WFD_ERR_CUDA, std::string("wavefieldsep_NoAlloc: shared memory for the tables: ") +
+                                                        cudaGetErrorString(e));
+                return WFD_ERR_CUDA;
+            }
+            k_sep_tables<<<1, 1024, smem, s>>>(n, m, scratch);
+            g_tables_n[dev] = n;
+        }
     }
     wfd::Grid g{};
     g.ndim = ny > 1 ? 3 : 2;
@@ -151,9 +171,16 @@ extern "C" int WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(long nx, long ny
     F.b = const_cast<float *>(b);
     F.pold = const_cast<float *>(pOld);
     F.mold = const_cast<float *>(mOld);
-    wfd_fast::image_wavefieldsep_tables(g, isFWI, F, wavefieldDP, wavefieldDM, dVel, scratch, m, s);
+    // the bitwise-parity build when WAVEFD_B200_STRICT=1, as for new propagator objects
+    const char *mode = getenv("WAVEFD_B200_STRICT");
+    if (mode && mode[0] == '1')
+        wfd_strict::image_wavefieldsep_tables(g, isFWI, F, wavefieldDP, wavefieldDM, dVel, scratch, m, s);
+    else
+        wfd_fast::image_wavefieldsep_tables(g, isFWI, F, wavefieldDP, wavefieldDM, dVel, scratch, m, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_tables_n[dev] = 0;  // the tables may not have been built
         wfd::set_global_error(WFD_ERR_CUDA, std::string("wavefieldsep_NoAlloc launch: ") + cudaGetErrorString(e));
         return WFD_ERR_CUDA;
     }
