@@ -288,6 +288,13 @@ const char *WFD_LastErrorMessage(void);
 int WFD_Prop_Status(void *p);
 const char *WFD_Prop_Message(void *p);
 
+/* Failure-detection hook (no counterpart in the reference): the limit, in ns, of the waits of the TMA
+ * step kernels for their tile loads (default 2 s; 0 restores it). A wait that runs out makes the
+ * kernel record a timeout in its device status word, let its copies in flight land and leave; the
+ * object then reports WFD_ERR_TIMEOUT. Tests shorten the limit to make a wait run out. Device-wide
+ * and synchronous; not for use while other work runs. */
+int WFD_Debug_SetPipelineWait(unsigned long long ns);
+
 /* 1 = bitwise-parity kernels (IEEE order, no FMA), 0 = fast kernels (default) */
 int WFD_Prop_SetStrict(void *p, int strict);
 /* 1 = fused single-sweep step kernels where available (default), 0 = the two-pass kernels */
@@ -304,6 +311,23 @@ void *WFD_Prop_Stream(void *p);
  * after WFD_Prop_Run, the launches per step of its loop (step kernels, the injection unless the step
  * kernel applied it, the extraction) */
 int WFD_Prop_StepKernels(void *p);
+/* kernels launched by the last WFD_Prop_Run (one for a 2D Iso loop run as a single cooperative launch) */
+long WFD_Prop_RunLaunches(void *p);
+/* No counterpart in the reference as one call: TimeStep followed by ForwardBornInjection_V
+ * (WFD_Prop_TimeStepBorn) or by AdjointBornAccumulation_V (WFD_Prop_TimeStepImage), with the
+ * reference's arithmetic for each (prop3DAcoIsoDenQ_DEO2_FDTD.h:305-334 / :518-546,
+ * prop3DAcoVTIDenQ_DEO2_FDTD.h:420-452 / :564-589, prop3DAcoTTIDenQ_DEO2_FDTD.h:423-452 / :567-592).
+ * The 3D step kernels apply them to each cell as they write it, so the fields cross HBM once; 2D
+ * objects run the separate kernels after the step. The imaging condition's pOld/mOld are the
+ * step's input pCur/mCur, as they are after the reference's TimeStep. wavefieldDM is required for
+ * VTI/TTI, ignored for Iso. linear != 0 (VTI only): the step is TimeStepLinear, as the reference's
+ * adjoint propagation uses. Device or managed arrays only; asynchronous on the object's stream. */
+int WFD_Prop_TimeStepBorn(void *p, const float *dVel, const float *wavefieldDP, const float *wavefieldDM);
+int WFD_Prop_TimeStepImage(void *p, float *dVel, const float *wavefieldDP, const float *wavefieldDM, int linear);
+/* No counterpart in the reference as one call: TimeStep followed by ScaleSpatialDerivatives (3D Iso
+ * .h:269-291, VTI .h:384-407, TTI .h:387-415): the 3D step kernels write pSpace (mSpace) already
+ * multiplied by V^2/B. Asynchronous on the object's stream. */
+int WFD_Prop_TimeStepScaled(void *p);
 /* Source illumination fused into the time step: with a device sum attached (ncells floats), every
  * later step adds pCur^2 (the field the step reads) to it, as illum_accumulate_float would; the 3D
  * Iso, VTI and TTI step kernels (nz a multiple of 4) do it in place of a separate pass. NULL
@@ -311,8 +335,11 @@ int WFD_Prop_StepKernels(void *p);
 int WFD_Prop_SetIllumination(void *p, float *accum);
 /* nsteps time steps of the object (TimeStep, then injection into pCur at time index it, then
  * extraction of pCur at it, it = it0, it0+1, ...; either table may be NULL), with every pair of steps
- * replayed from one CUDA graph when use_graph != 0; indices beyond nt are skipped. Enqueued on the
- * object's stream; returns after the graph launches are complete. */
+ * replayed from one CUDA graph when use_graph != 0; indices beyond nt are skipped. A 2D Iso object
+ * (fused kernels, no illumination sum, at most 1024 source groups) runs the whole loop as one
+ * cooperative launch instead, with a grid-wide barrier between steps (bounded: a barrier that waits
+ * longer than 2 s returns WFD_ERR_TIMEOUT). Enqueued on the object's stream; returns after the
+ * launches are complete. */
 int WFD_Prop_Run(void *p, long nsteps, long it0, void *src_table, const float *wavelet, void *rec_table,
                  float *traces, long nt, int use_graph);
 /* device-resident source/receiver tables built from a flat point list (grouped by written
@@ -435,9 +462,12 @@ int WFD_Codec_Gradient(void *codec, const float *blocks, long n, float *grad, fl
  * z fastest; ny = 1 for 2D; wavefieldDM and mOld both NULL for the isotropic case); dVel is
  * accumulated. Its FFT scratch is a fixed 160 KiB device array inside the library, so nz is
  * limited to 2048 (larger nz returns WFD_ERR_ARG). The first call on each device looks up that
- * array's device address; make that first call before any stream capture. All calls share the
- * array: calls that overlap on the GPU race. Work is enqueued on `stream` (a cudaStream_t, NULL
- * for the default stream) without host synchronisation. Returns a WFD_* status. */
+ * array's device address; make that first call before any stream capture, and do not use the
+ * entry point across a cudaDeviceReset. The image must be on the current device. All calls share
+ * the array (it keeps the tables of the last FFT length): calls that overlap on the GPU race. The
+ * arithmetic is the fast build's, or the bitwise-parity build's when WAVEFD_B200_STRICT=1 (as for
+ * new propagator objects). Work is enqueued on `stream` (a cudaStream_t, NULL for the default
+ * stream) without host synchronisation. Returns a WFD_* status. */
 int WFD_AdjointBornAccumulation_wavefieldsep_NoAlloc(long nx, long ny, long nz, long isFWI, const float *v,
                                                      const float *b, const float *wavefieldDP, const float *pOld,
                                                      const float *wavefieldDM, const float *mOld, float *dVel,

@@ -50,6 +50,11 @@ def _declare(lib):
     fn("WFD_Prop_Prefetch", c_int, [c_void_p])
     fn("WFD_Prop_Stream", c_void_p, [c_void_p])
     fn("WFD_Prop_StepKernels", c_int, [c_void_p])
+    fn("WFD_Prop_RunLaunches", c_long, [c_void_p])
+    fn("WFD_Prop_TimeStepBorn", c_int, [c_void_p, c_void_p, c_void_p, c_void_p])
+    fn("WFD_Prop_TimeStepImage", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int])
+    fn("WFD_Prop_TimeStepScaled", c_int, [c_void_p])
+    fn("WFD_Debug_SetPipelineWait", c_int, [ctypes.c_ulonglong])
     fn("WFD_Points_Create", c_void_p, [POINTER(SourcePoint32), c_long, c_int])
     fn("WFD_Points_Free", None, [c_void_p])
     fn("WFD_Points_Groups", c_long, [c_void_p])

@@ -31,7 +31,8 @@ STRICT = ["-DWFD_STRICT=1", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", 
 FAST = ["-DWFD_STRICT=0", "-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 
 KERNEL_SOURCES = ["wfd_generic.cu", "wfd_fused.cu", "wfd_fused_iso3d.cu", "wfd_fused_iso3d_tma.cu",
-                  "wfd_fused_aniso3d_tma.cu", "wfd_fused_vti3d_tma.cu", "wfd_fused_iso2d.cu", "wfd_wavefieldsep.cu"]
+                  "wfd_fused_aniso3d_tma.cu", "wfd_fused_vti3d_tma.cu", "wfd_fused_iso2d.cu", "wfd_fused_aniso2d.cu",
+                  "wfd_wavefieldsep.cu"]
 HOST_SOURCES = ["wfd_prop.cu", "wfd_bornimage.cu", "wfd_capi.cu", "wfd_addon.cu", "wfd_spacetime.cu",
                 "wfd_tma_host.cu", "wfd_noalloc.cu", "wfd_batch.cu", "wfd_codec.cu", "wfd_interp.cu", "wfd_illum.cu", "wfd_snapio.cu"]
 

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_points.h"
 #include "wfd_prop.h"
 
@@ -241,10 +242,10 @@ int plan_group(Batch *b, Group &G) {
     cudaFree(G.d_items);
     G.d_desc = nullptr;
     G.d_items = nullptr;
-    if (int rc = bcheck(b, cudaMalloc(&G.d_desc, host.size()), "descriptor allocation")) return rc;
-    if (int rc = bcheck(b, cudaMalloc(&G.d_items, sizeof(int2) * hitems.size()), "item allocation")) return rc;
+    if (int rc = bcheck(b, wfd::dMalloc(&G.d_desc, host.size()), "descriptor allocation")) return rc;
+    if (int rc = bcheck(b, wfd::dMalloc(&G.d_items, sizeof(int2) * hitems.size()), "item allocation")) return rc;
     if (!G.d_sel)
-        if (int rc = bcheck(b, cudaMalloc(&G.d_sel, sizeof(int) * 2 * ns), "selector allocation")) return rc;
+        if (int rc = bcheck(b, wfd::dMalloc(&G.d_sel, sizeof(int) * 2 * ns), "selector allocation")) return rc;
     cudaMemcpy(G.d_desc, host.data(), host.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(G.d_items, hitems.data(), sizeof(int2) * hitems.size(), cudaMemcpyHostToDevice);
     G.nitems = (int)hitems.size();
@@ -278,11 +279,11 @@ int build_pointset(Batch *b, PointSet &ps, bool receivers) {
     start.push_back(base);
     ps.ngroups = (long)key.size();
     if (!ps.ngroups) return WFD_OK;
-    bool ok = cudaMalloc(&ps.d_shot, sizeof(int) * shot.size()) == cudaSuccess &&
-              cudaMalloc(&ps.d_key, sizeof(long) * key.size()) == cudaSuccess &&
-              cudaMalloc(&ps.d_start, sizeof(long) * start.size()) == cudaSuccess &&
-              cudaMalloc(&ps.d_other, sizeof(long) * other.size()) == cudaSuccess &&
-              cudaMalloc(&ps.d_c, sizeof(float) * c.size()) == cudaSuccess;
+    bool ok = wfd::dMalloc(&ps.d_shot, sizeof(int) * shot.size()) == cudaSuccess &&
+              wfd::dMalloc(&ps.d_key, sizeof(long) * key.size()) == cudaSuccess &&
+              wfd::dMalloc(&ps.d_start, sizeof(long) * start.size()) == cudaSuccess &&
+              wfd::dMalloc(&ps.d_other, sizeof(long) * other.size()) == cudaSuccess &&
+              wfd::dMalloc(&ps.d_c, sizeof(float) * c.size()) == cudaSuccess;
     if (!ok) return bfail(b, WFD_ERR_ALLOC, "point table allocation failed");
     cudaMemcpy(ps.d_shot, shot.data(), sizeof(int) * shot.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(ps.d_key, key.data(), sizeof(long) * key.size(), cudaMemcpyHostToDevice);
@@ -519,7 +520,7 @@ int batch_tune(Batch *b, int reps) {
     size_t total = 0;
     for (int s = 0; s < n; s++) total += written_arrays(b, s).size() * (size_t)b->props[s]->ncells();
     float *save = nullptr;
-    if (int rc = bcheck(b, cudaMalloc(&save, sizeof(float) * total), "tuner save area")) return rc;
+    if (int rc = bcheck(b, wfd::dMalloc(&save, sizeof(float) * total), "tuner save area")) return rc;
     auto copy_all = [&](bool out) {
         size_t off = 0;
         for (int s = 0; s < n; s++) {
@@ -672,11 +673,11 @@ Batch *batch_create(Prop *const *props, long n) {
              cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreate(&b->ev_t0) == cudaSuccess && cudaEventCreate(&b->ev_t1) == cudaSuccess &&
-         cudaMalloc(&b->d_counter, sizeof(int) * 3) == cudaSuccess &&
-         cudaMalloc(&b->d_it, sizeof(long)) == cudaSuccess &&
-         cudaMalloc(&b->d_fieldp, sizeof(float *) * 2 * n) == cudaSuccess &&
-         cudaMalloc(&b->d_datap, sizeof(float *) * 2 * n) == cudaSuccess &&
-         cudaMalloc(&b->d_nt, sizeof(long) * n) == cudaSuccess;
+         wfd::dMalloc(&b->d_counter, sizeof(int) * 3) == cudaSuccess &&
+         wfd::dMalloc(&b->d_it, sizeof(long)) == cudaSuccess &&
+         wfd::dMalloc(&b->d_fieldp, sizeof(float *) * 2 * n) == cudaSuccess &&
+         wfd::dMalloc(&b->d_datap, sizeof(float *) * 2 * n) == cudaSuccess &&
+         wfd::dMalloc(&b->d_nt, sizeof(long) * n) == cudaSuccess;
     if (!ok) {
         set_global_error(WFD_ERR_ALLOC, "WFD_Batch_Create: device resources");
         batch_destroy(b);

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "wfd_prop.h"
+#include "wfd_alloc.h"
 
 namespace wfd {
 
@@ -33,11 +34,8 @@ struct Staged {
 class Stager {
   public:
     explicit Stager(Prop *p) : p_(p) {}
-    ~Stager() {
-        for (auto &s : v_)
-            if (s.copied && s.dev) cudaFreeAsync(s.dev, p_->stream);
-    }
-    // map a caller array of ncells floats; copy host contents in
+    // map a caller array of ncells floats; copy host contents in. Host arrays go through the
+    // object's staging buffers, allocated on first use and kept for its later calls.
     float *in(float *user) {
         Staged s;
         s.user = user;
@@ -45,11 +43,17 @@ class Stager {
         if (device_accessible(user)) {
             s.dev = user;
         } else {
-            const size_t bytes = sizeof(float) * (size_t)p_->ncells();
-            if (cudaMallocAsync(&s.dev, bytes, p_->stream) != cudaSuccess) {
+            if (next_ >= (int)(sizeof(p_->stage) / sizeof(p_->stage[0]))) {
                 ok_ = false;
                 return nullptr;
             }
+            const size_t bytes = sizeof(float) * (size_t)p_->ncells();
+            if (!p_->stage[next_] && wfd::dMalloc(&p_->stage[next_], bytes) != cudaSuccess) {
+                p_->stage[next_] = nullptr;
+                ok_ = false;
+                return nullptr;
+            }
+            s.dev = p_->stage[next_++];
             cudaMemcpyAsync(s.dev, user, bytes, cudaMemcpyHostToDevice, p_->stream);
             s.copied = true;
         }
@@ -68,6 +72,7 @@ class Stager {
   private:
     Prop *p_;
     std::vector<Staged> v_;
+    int next_ = 0;
     bool ok_ = true;
 };
 
@@ -166,7 +171,7 @@ int prop_image(Prop *p, const char *variant, float *const *args, int nargs, long
         const long nfft = 2 * g.nz;
         if (!p->work) {
             long cols = ncols < 4096 ? ncols : 4096;
-            if (cudaMalloc(&p->work, sizeof(float2) * (size_t)cols * (size_t)nfft * 2) != cudaSuccess)
+            if (wfd::dMalloc(&p->work, sizeof(float2) * (size_t)cols * (size_t)nfft * 2) != cudaSuccess)
                 return prop_fail(p, WFD_ERR_ALLOC, "FFT workspace allocation failed");
             p->work_cols = cols;
         }
@@ -251,6 +256,10 @@ void apply_dplus2d(bool fs, long nx, long nz, float c1, float c2, float c3, floa
     }
     cudaError_t e = cudaStreamSynchronize(tmp.stream);
     if (e != cudaSuccess) set_global_error(WFD_ERR_CUDA, cudaGetErrorString(e));
+    for (float *&b : tmp.stage) {
+        if (b) cudaFree(b);
+        b = nullptr;
+    }
     cudaStreamDestroy(tmp.stream);
     tmp.stream = nullptr;
 }

@@ -39,6 +39,7 @@
 #include <vector>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_prop.h"
 
 namespace wfd {
@@ -867,10 +868,10 @@ extern "C" void *WFD_Codec_Create(unsigned seed) {
     Codec *c = new Codec();
     cudaGetDevice(&c->device);
     const size_t nb = sizeof(float) * NPARAM;
-    bool ok = cudaMalloc(&c->w, nb) == cudaSuccess && cudaMalloc(&c->m, nb) == cudaSuccess &&
-              cudaMalloc(&c->v, nb) == cudaSuccess && cudaMalloc(&c->grad, nb) == cudaSuccess &&
-              cudaMalloc(&c->loss, sizeof(float)) == cudaSuccess &&
-              cudaMalloc(&c->wb, sizeof(bf16) * NPARAM) == cudaSuccess;
+    bool ok = wfd::dMalloc(&c->w, nb) == cudaSuccess && wfd::dMalloc(&c->m, nb) == cudaSuccess &&
+              wfd::dMalloc(&c->v, nb) == cudaSuccess && wfd::dMalloc(&c->grad, nb) == cudaSuccess &&
+              wfd::dMalloc(&c->loss, sizeof(float)) == cudaSuccess &&
+              wfd::dMalloc(&c->wb, sizeof(bf16) * NPARAM) == cudaSuccess;
     if (!ok) {
         wfd::set_global_error(WFD_ERR_ALLOC, "WFD_Codec_Create: device allocation failed");
         cudaFree(c->w), cudaFree(c->m), cudaFree(c->v), cudaFree(c->grad), cudaFree(c->loss), cudaFree(c->wb);

@@ -47,13 +47,24 @@ __device__ __forceinline__ float stm(const Grid &g, const W &w) {
 constexpr int WZ = 32, WX = NT / WZ;
 static_assert(NT % WZ == 0 && TZ % WZ == 0, "thread layout");
 
-__global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
-    __shared__ float P[PXH][PZW];
-    __shared__ float Bs[BXH][BZW];
-    __shared__ float T0[T0H][TZ];
-    __shared__ float T2[TX][T2W];
+struct Tile {
+    float P[PXH][PZW];
+    float Bs[BXH][BZW];
+    float T0[T0H][TZ];
+    float T2[TX][T2W];
+};
+
+// One step of the tile at (x0, z0): F.pcur -> F.pold, F.pspace; then the source injection F.inj at
+// time index it into the tile's cells of the new field (nothing when it is outside 1..nt). Ends with
+// the tile's writes done by every thread of the CTA only if injecting (callers reusing the shared
+// memory synchronise first).
+__device__ __forceinline__ void tile_step(const Grid &g, const Fields &F, const long x0, const long z0, const long it,
+                                          Tile &sm) {
+    auto &P = sm.P;
+    auto &Bs = sm.Bs;
+    auto &T0 = sm.T0;
+    auto &T2 = sm.T2;
     const int tz = threadIdx.x % WZ, tx = threadIdx.x / WZ;
-    const long z0 = (long)blockIdx.x * TZ, x0 = (long)blockIdx.y * TX;
     const long nx = g.nx, nz = g.nz;
 
     // pCur with its antisymmetric image above kz = 0 (zero outside the grid elsewhere)
@@ -159,7 +170,6 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     // tile, after the tile's cells are written (visible to the CTA after the barrier); each group's
     // contributions in order, separate IEEE multiply and add, as the injection kernel does
     if (F.inj.ngroups) {
-        const long it = *F.inj.d_it;
         if (it >= 1 && it <= F.inj.nt) {
             __syncthreads();
             for (long gi = threadIdx.x; gi < F.inj.ngroups; gi += NT) {
@@ -175,7 +185,114 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     }
 }
 
+
+__global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
+    __shared__ Tile sm;
+    const long it = F.inj.ngroups ? *F.inj.d_it : 0;
+    tile_step(g, F, (long)blockIdx.y * TX, (long)blockIdx.x * TZ, it, sm);
+}
+
+// Grid-wide barrier of the persistent run (all CTAs co-resident: cooperative launch). Sense by
+// generation: the last CTA to arrive resets the count and publishes the next generation. Every wait
+// is bounded (2 s): a CTA that gives up, or sees that another gave up, sets the status word and
+// returns false, and so does every CTA after it, so the kernel always ends.
+__device__ __forceinline__ bool grid_barrier(unsigned *words, unsigned &gen, int *ok_flag) {
+    unsigned *count = words, *pub = words + 1, *status = words + 2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned target = gen + 1;
+        __threadfence();
+        if (atomicAdd(count, 1u) + 1 == gridDim.x) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicExch(pub, target);
+        } else {
+            uint64_t t0;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+            while (*(volatile unsigned *)pub != target) {
+                if (*(volatile unsigned *)status) {
+                    ok = 0;
+                    break;
+                }
+                uint64_t t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                if (t - t0 > 2000000000ull) {
+                    atomicOr(status, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        gen = target;
+        *ok_flag = ok;
+    }
+    __syncthreads();
+    return *ok_flag != 0;
+}
+
+// A whole time loop in one launch: nsteps steps, each followed by its source injection (in the step,
+// per tile) and, after a grid-wide barrier, its receiver extraction from the new field, at time
+// indices it0, it0+1, ...; the pointer swap of every step is the alternation of F.pcur and F.pold.
+// Between two steps one barrier suffices: step s+1 writes only the array step s read (every read of
+// it is done before the barrier), and the extraction of step s reads the array step s+1 only reads.
+__global__ void __launch_bounds__(NT) k_iso2d_run(Grid g, Fields F, long nsteps, long it0, RunExtract ex,
+                                                  unsigned *sync_words) {
+    __shared__ Tile sm;
+    __shared__ int ok_flag;
+    const long ntz = (g.nz + TZ - 1) / TZ, ntx = (g.nx + TX - 1) / TX, ntiles = ntz * ntx;
+    float *A = F.pcur, *B = F.pold;
+    unsigned gen = 0;
+    for (long st = 0; st < nsteps; st++) {
+        Fields Fs = F;
+        Fs.pcur = (st & 1) ? B : A;
+        Fs.pold = (st & 1) ? A : B;
+        const long it = it0 + st;
+        for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            tile_step(g, Fs, (t / ntz) * TX, (t % ntz) * TZ, it, sm);
+            __syncthreads();  // the tile's shared memory is reused by the next tile
+        }
+        if (!grid_barrier(sync_words, gen, &ok_flag)) return;
+        if (ex.ngroups && it >= 1 && it <= ex.nt) {
+            // data[key*nt + it-1] += sum c * new field[other], each group in order, IEEE multiply and add
+            for (long gi = (long)blockIdx.x * NT + threadIdx.x; gi < ex.ngroups; gi += (long)gridDim.x * NT) {
+                float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
+                float acc = *dst;
+                for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], Fs.pold[ex.other[j]]));
+                *dst = acc;
+            }
+        }
+    }
+}
 }  // namespace
+
+int iso2d_run(const Grid &g, const Fields &F, long nsteps, long it0, const RunExtract &ex, unsigned *sync_words,
+              cudaStream_t s) {
+    if (g.ndim != 2) return -1;
+    static int cap = 0;
+    if (!cap) {
+        int dev = 0, sms = 0, per = 0, coop = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_iso2d_run, NT, 0);
+        cap = coop && per > 0 ? sms * per : -1;
+    }
+    if (cap <= 0) return -1;
+    const long ntiles = ((g.nz + TZ - 1) / TZ) * ((g.nx + TX - 1) / TX);
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    Grid gg = g;
+    Fields FF = F;
+    long ns = nsteps, i0 = it0;
+    RunExtract ee = ex;
+    unsigned *sw = sync_words;
+    void *args[] = {&gg, &FF, &ns, &i0, &ee, &sw};
+    return cudaLaunchCooperativeKernel((const void *)k_iso2d_run, dim3(grid), dim3(NT), args, 0, s) == cudaSuccess ? 0
+                                                                                                                   : 1;
+}
 
 bool fused_iso2d(const Grid &g, const Fields &F, cudaStream_t s) {
     if (g.ndim != 2) return false;

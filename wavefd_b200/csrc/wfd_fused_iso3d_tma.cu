@@ -58,6 +58,8 @@ __device__ unsigned int d_status;
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
 __device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float at(const float4 &v, int i) {
     return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
@@ -222,7 +224,8 @@ template <int MODE>
 __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const bool xin, const bool top, const int z,
                                           const int y, const unsigned fmask, const int zq, const int row,
                                           const float2 *sx, const float2 *pc, const float *st, const float *TYs,
-                                          const float *TZs, float *po, float *ps, float *illum) {
+                                          const float *TZs, float *po, float *ps, float *illum,
+                                          const StepEpilogue *epi) {
     const int o = row * TZ + 4 * zq;
     const float4 pold4 = ld4(st + S_PO + o), v4 = ld4(st + S_V + o), q4 = ld4(st + S_Q + o);
     const float4 b4 = ld4(st + S_BH + (4 + row) * BZW + 4 + 4 * zq);
@@ -278,6 +281,23 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
         if (MODE != INNER) {
             np = keep2(fm, m0, np, pov);  // cells the reference leaves alone
             nl = keep2(fm, m0, nl, bc2(0.0f));
+        }
+        if (epi && epi->scale_space)  // ScaleSpatialDerivatives fused (.h:269-291): pSpace *= V^2/B
+            nl = mul2(nl, div2(mul2(V, V), half2(b4, h)));
+        if (epi && epi->born_dv) {
+            // Born-V injection fused after the step (prop3DAcoIsoDenQ_DEO2_FDTD.h:305-334), every cell:
+            // new += dt^2 V^2/B * DP * (2 B dV / V^3)
+            const long kc = j * g.sx + (long)y * g.nz + z + m0;
+            const float2 B = half2(b4, h);
+            const float2 fv = div2(mul2(mul2(bc2(2.0f), B), ld2(epi->born_dv + kc)), mul2(mul2(V, V), V));
+            np = add2(np, mul2(mul2(k2, ld2(epi->born_dp + kc)), fv));
+        }
+        if (epi && epi->img) {
+            // imaging condition fused after the step (.h:518-546): img += 2B/V^3 DP pOld, pOld being
+            // this step's input pCur
+            const long kc = j * g.sx + (long)y * g.nz + z + m0;
+            const float2 fv = div2(mul2(bc2(2.0f), half2(b4, h)), mul2(mul2(V, V), V));
+            st2(epi->img + kc, add2(ld2(epi->img + kc), mul2(mul2(fv, ld2(epi->img_dp + kc)), pcv)));
         }
         npo[h] = np;
         nps[h] = nl;
@@ -448,11 +468,13 @@ __global__ void __launch_bounds__(NT, 3)
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
             }
-            if (!mbar_wait(&bars[slot], par)) {
+            const bool landed = mbar_wait(&bars[slot], par);
+            if (!landed) {
                 atomicExch(abort_flag, 1);
                 atomicOr(&d_status, 1u);
             }
-            if (tid == 0) out_from = gs + 1;
+            // a group whose wait ran out may still be in flight: the drain below waits for it
+            if (tid == 0 && landed) out_from = gs + 1;
             const float *st = sm + slot * STAGE;
             slot = slot + 1 == NS ? 0u : slot + 1;
             par ^= slot == 0 ? 1u : 0u;
@@ -479,7 +501,7 @@ __global__ void __launch_bounds__(NT, 3)
                 ext_stage<EDGE>(g, xin, tile_top, z0, emask, st, TYs, TZs);
                 __syncthreads();
                 if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, fmask, zq, row, sx, pc, st, TYs, TZs, out_pold,
-                                          out_pspace, BATCH ? nullptr : F.illum);
+                                          out_pspace, BATCH ? nullptr : F.illum, BATCH ? nullptr : &F.epi);
             }
             __syncthreads();
             if (*abort_flag) {
@@ -582,6 +604,11 @@ void iso3d_tma_batch(const Grid &gc, const IsoShotDesc *shots, const int *sel, c
                      int *counter, int grid, cudaStream_t s) {
     k_iso3d_tma<true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, IsoMaps{}, 0, 0, 0, 1, shots, sel, items, nitems,
                                                    counter);
+}
+
+void iso3d_set_pipeline_wait(unsigned long long ns) {
+    const uint64_t v = ns;
+    cudaMemcpyToSymbol(wfd_dev::d_pipeline_wait_ns, &v, sizeof(v));
 }
 
 unsigned iso3d_status_and_clear() {

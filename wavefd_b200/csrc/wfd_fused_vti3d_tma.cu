@@ -392,11 +392,13 @@ __global__ void __launch_bounds__(NT, 2)
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
             }
-            if (!mbar_wait(&bars[gs % NS], (gs / NS) & 1u)) {
+            const bool landed = mbar_wait(&bars[gs % NS], (gs / NS) & 1u);
+            if (!landed) {
                 atomicExch(abort_flag, 1);
                 atomicOr(&d_status, 1u);
             }
-            if (tid == ISSUER) out_from = gs + 1;
+            // a group whose wait ran out may still be in flight: the drain below waits for it
+            if (tid == ISSUER && landed) out_from = gs + 1;
             const float *st = sm + (gs % NS) * STAGE;
             float2 sx[2], pc[2];
             {
@@ -457,14 +459,38 @@ __global__ void __launch_bounds__(NT, 2)
                     const float2 B = ld2(st + S_BH + (row + 4) * MZW + 4 + 2 * zp);
                     const float2 k2 = div2(mul2(mul2(bc2(g.dt2), V), V), B);
                     const long k = j * g.sx + (long)y * g.nz + z;
+                    // Born-V injection fused after the step (prop3DAcoVTIDenQ_DEO2_FDTD.h:420-452):
+                    // new += 2 dt^2 dV/V * DP (DM), every cell
+                    float2 bfac = bc2(0.0f);
+                    if (!BATCH && F.epi.born_dv)
+                        bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), __ldg(reinterpret_cast<const float2 *>(F.epi.born_dv + k))), V);
 #pragma unroll
                     for (int f = 0; f < 2; f++) {
                         const float2 po = ld2(st + (f == 0 ? S_PO : S_MO) + o);
                         const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc[f], po))), po);
                         const float2 np = add2(t, mul2(bc2(2.0f), pc[f]));
-                        st2((f == 0 ? o_po : o_mo) + k, make_float2(ok0 ? np.x : po.x, ok1 ? np.y : po.y));
-                        if (!LINEAR)
-                            st2((f == 0 ? o_ps : o_ms) + k, make_float2(ok0 ? L[f].x : 0.0f, ok1 ? L[f].y : 0.0f));
+                        float2 nv = make_float2(ok0 ? np.x : po.x, ok1 ? np.y : po.y);
+                        if (!BATCH && F.epi.born_dv) {
+                            const float *d = f == 0 ? F.epi.born_dp : F.epi.born_dm;
+                            nv = add2(nv, mul2(bfac, __ldg(reinterpret_cast<const float2 *>(d + k))));
+                        }
+                        st2((f == 0 ? o_po : o_mo) + k, nv);
+                        if (!LINEAR) {
+                            float2 sp = make_float2(ok0 ? L[f].x : 0.0f, ok1 ? L[f].y : 0.0f);
+                            // ScaleSpatialDerivatives fused (.h:384-407): pSpace, mSpace *= V^2/B
+                            if (!BATCH && F.epi.scale_space) sp = mul2(sp, div2(mul2(V, V), B));
+                            st2((f == 0 ? o_ps : o_ms) + k, sp);
+                        }
+                    }
+                    if (!BATCH && F.epi.img) {
+                        // imaging condition fused after the step (.h:564-589): img += 2B/V^3 (DP pOld +
+                        // DM mOld), pOld/mOld being this step's input pCur/mCur
+                        const float2 dp = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dp + k));
+                        const float2 dm = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dm + k));
+                        const float2 fac = div2(mul2(bc2(2.0f), B), mul2(mul2(V, V), V));
+                        float2 a = ld2(F.epi.img + k);
+                        a = add2(a, mul2(fac, add2(mul2(dp, pc[0]), mul2(dm, pc[1]))));
+                        st2(F.epi.img + k, a);
                     }
                     if (!BATCH && F.illum) {
                         // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and
@@ -581,6 +607,11 @@ void vti3d_tma_batch(const Grid &gc, const AnisoShotDesc *shots, const int *sel,
     vti_grid_cap<false>();
     k_vti3d_tma<false, true><<<grid, NT, SMEM_BYTES, s>>>(gc, Fields{}, AnisoMaps{}, 0, 0, 0, 1, shots, sel, items,
                                                          nitems, counter);
+}
+
+void vti3d_set_pipeline_wait(unsigned long long ns) {
+    const uint64_t v = ns;
+    cudaMemcpyToSymbol(wfd_dev::d_pipeline_wait_ns, &v, sizeof(v));
 }
 
 unsigned vti3d_status_and_clear() {

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_prop.h"
 
 namespace wfd {
@@ -43,8 +44,8 @@ void dropin(T *accum, T *field, size_t n) {
     const bool fdev = device_accessible(field), adev = !accum || device_accessible(accum);
     T *df = fdev ? field : nullptr, *da = (accum && adev) ? accum : nullptr;
     bool ok = true;
-    if (!fdev) ok = cudaMallocAsync(&df, sizeof(T) * n, s) == cudaSuccess;
-    if (ok && accum && !adev) ok = cudaMallocAsync(&da, sizeof(T) * n, s) == cudaSuccess;
+    if (!fdev) ok = wfd::dMallocAsync(&df, sizeof(T) * n, s) == cudaSuccess;
+    if (ok && accum && !adev) ok = wfd::dMallocAsync(&da, sizeof(T) * n, s) == cudaSuccess;
     if (!ok) {
         set_global_error(WFD_ERR_ALLOC, "illumination: device allocation failed");
     } else {

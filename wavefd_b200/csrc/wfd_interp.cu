@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_points.h"
 #include "wfd_prop.h"
 
@@ -134,9 +135,9 @@ void dropin(int forward, T **h, T *out, const T *in, size_t nh, size_t nm, size_
     const size_t nout = (forward ? nd : nm) * nslow, nin = (forward ? nm : nd) * nslow;
     T *dh = nullptr, *dout = nullptr, *din = nullptr;
     const bool out_dev = device_accessible(out), in_dev = device_accessible(in);
-    bool ok = cudaMallocAsync(&dh, sizeof(T) * ht.size(), s) == cudaSuccess;
-    if (ok && !out_dev) ok = cudaMallocAsync(&dout, sizeof(T) * (nout ? nout : 1), s) == cudaSuccess;
-    if (ok && !in_dev) ok = cudaMallocAsync(&din, sizeof(T) * (nin ? nin : 1), s) == cudaSuccess;
+    bool ok = wfd::dMallocAsync(&dh, sizeof(T) * ht.size(), s) == cudaSuccess;
+    if (ok && !out_dev) ok = wfd::dMallocAsync(&dout, sizeof(T) * (nout ? nout : 1), s) == cudaSuccess;
+    if (ok && !in_dev) ok = wfd::dMallocAsync(&din, sizeof(T) * (nin ? nin : 1), s) == cudaSuccess;
     if (!ok) {
         set_global_error(WFD_ERR_ALLOC, "time interpolation: device allocation failed");
     } else {

@@ -23,11 +23,39 @@ struct StepInject {
     const long *d_it;
 };
 
+// Work fused into the end of a 3D step (single objects; a null pointer turns it off), each cell as
+// the reference computes it, so that the arrays cross HBM once:
+// * born: ForwardBornInjection_V applied to the new fields right after the step (3D Iso
+//   prop3DAcoIsoDenQ_DEO2_FDTD.h:305-334: p += dt^2 V^2/B DP (2B dV/V^3); VTI/TTI .h:420-452 /
+//   :423-452: p += 2 dt^2 dV/V DP, m += 2 dt^2 dV/V DM);
+// * image: AdjointBornAccumulation_V right after the step, whose pOld/mOld are the step's input
+//   pCur/mCur (3D Iso .h:518-546: img += 2B/V^3 DP pOld; VTI/TTI .h:564-589 / :567-592:
+//   img += 2B/V^3 (DP pOld + DM mOld)).
+// * scale_space: ScaleSpatialDerivatives right after the step (3D Iso .h:269-291, VTI .h:384-407, TTI
+//   .h:387-415): pSpace (and mSpace) written already multiplied by V^2/B.
+struct StepEpilogue {
+    const float *born_dv, *born_dp, *born_dm;
+    float *img;
+    const float *img_dp, *img_dm;
+    int scale_space;
+};
+
+// Receiver extraction inside a persistent time loop: data[key[g]*nt + it-1] += c[j] * field[other[j]]
+// for j = start[g] .. start[g+1]-1 in order, each product and sum rounded (IEEE).
+struct RunExtract {
+    long ngroups;
+    const long *key, *start, *other;
+    const float *c;
+    float *data;
+    long nt;
+};
+
 struct Fields {
     float *v, *b, *q, *eps, *eta, *f, *st, *ct, *sp, *cp;
     float *pcur, *pold, *pspace, *mcur, *mold, *mspace;
     float *illum;  // source illumination sum (sum over steps of pCur^2), or nullptr
     StepInject inj;
+    StepEpilogue epi;
 };
 
 // Scratch of the unfused passes (the reference's tmp arrays), device memory.
@@ -73,7 +101,8 @@ struct TileInfo {
     void pass2(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, const wfd::Scratch &S,    \
                cudaStream_t s);                                                                          \
     /* fused single-sweep steps; 0 when the geometry is not handled, else flags: 1 stepped, 2 F.illum \
-       accumulated inside the step kernel, 4 F.inj applied inside the step kernel */                    \
+       accumulated inside the step kernel, 4 F.inj applied inside the step kernel, 8 F.epi applied  \
+       inside the step kernel */                                                                         \
     int fused_step(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);      \
     void scale(const wfd::Grid &g, const wfd::Fields &F, bool two, cudaStream_t s);                      \
     void dplus(const wfd::Grid &g, const float *in, float *ox, float *oy, float *oz, cudaStream_t s);    \
@@ -81,9 +110,14 @@ struct TileInfo {
                 float *oy, float *oz, cudaStream_t s);                                                   \
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
     bool fused_iso2d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
+    bool fused_aniso2d(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);  \
+    /* whole 2D Iso time loop in one cooperative launch: 0 launched, -1 not available, 1 launch error */ \
+    int iso2d_run(const wfd::Grid &g, const wfd::Fields &F, long nsteps, long it0, const wfd::RunExtract &ex, \
+                  unsigned *sync_words, cudaStream_t s);                                                 \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \
+    bool fused_tti3d_split(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                   \
     bool vti3d_tma_describe(const wfd::Grid &g, const wfd::Fields &F, int xchunk, wfd::AnisoShotDesc *d, \
                             wfd::TileInfo *t);                                                           \
     void vti3d_tma_batch(const wfd::Grid &gc, const wfd::AnisoShotDesc *shots, const int *sel,          \
@@ -102,6 +136,10 @@ struct TileInfo {
                            cudaStream_t s);                                                              \
     unsigned aniso3d_status_and_clear();                                                                 \
     unsigned fused_status_and_clear();                                                                   \
+    void iso3d_set_pipeline_wait(unsigned long long ns);                                                 \
+    void vti3d_set_pipeline_wait(unsigned long long ns);                                                 \
+    void aniso3d_set_pipeline_wait(unsigned long long ns);                                               \
+    void fused_set_pipeline_wait(unsigned long long ns);                                                 \
     void dminus3(const wfd::Grid &g, const float *fx, const float *fy, const float *fz, float *ox,       \
                  float *oy, float *oz, cudaStream_t s);                                                  \
     void tti_dplus(const wfd::Grid &g, const wfd::Fields &F, const float *in, float *o1, float *o2,      \

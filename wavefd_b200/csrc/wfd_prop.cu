@@ -1,6 +1,7 @@
 // Propagator objects: allocation (managed memory behind the getters), the Q/sponge profile,
 // and dispatch of the time step, Born injection and imaging conditions to the kernels.
 #include "wfd_prop.h"
+#include "wfd_alloc.h"
 
 #include <float.h>
 #include <math.h>
@@ -8,6 +9,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -29,6 +31,30 @@ bool uses(int phys, int ndim, int f) {
     }
 }
 }  // namespace
+
+// ---- allocation fault injector (wfd_alloc.h) ----------------------------------------------------
+namespace {
+std::atomic<long> g_alloc_count{0};
+thread_local const char *t_injected = "";
+
+long fail_at() {
+    static const long n = [] {
+        const char *e = getenv("WAVEFD_B200_FAIL_ALLOC");
+        return e && *e ? strtol(e, nullptr, 10) : 0L;
+    }();
+    return n;
+}
+}  // namespace
+
+bool alloc_should_fail() {
+    const long n = fail_at();
+    if (n <= 0) return false;
+    const bool fail = g_alloc_count.fetch_add(1) + 1 == n;
+    t_injected = fail ? " (injected: WAVEFD_B200_FAIL_ALLOC)" : "";
+    return fail;
+}
+
+const char *alloc_injected_note() { return t_injected; }
 
 void set_global_error(int code, const std::string &msg) {
     std::lock_guard<std::mutex> lk(g_err_mu);
@@ -99,6 +125,7 @@ Fields Prop::fields() const {
     F.mspace = field[F_MSPACE];
     F.illum = illum;
     F.inj = inj;
+    F.epi = epi;
     return F;
 }
 
@@ -112,10 +139,11 @@ bool ensure_scratch(Prop *p, int count) {
     const size_t bytes = sizeof(float) * (size_t)p->ncells();
     for (int i = 0; i < count && i < 12; i++) {
         if (p->tmp[i]) continue;
-        cudaError_t e = cudaMalloc(&p->tmp[i], bytes);
+        cudaError_t e = wfd::dMalloc(&p->tmp[i], bytes);
         if (e != cudaSuccess) {
             p->tmp[i] = nullptr;
-            prop_fail(p, WFD_ERR_ALLOC, std::string("scratch allocation failed: ") + cudaGetErrorString(e));
+            prop_fail(p, WFD_ERR_ALLOC,
+                      std::string("scratch allocation failed: ") + cudaGetErrorString(e) + alloc_injected_note());
             return false;
         }
         cudaMemsetAsync(p->tmp[i], 0, bytes, p->stream);
@@ -150,21 +178,26 @@ Prop *prop_create(int ndim, int phys, long fs, long nthread, long nx, long ny, l
     const char *fz = getenv("WAVEFD_B200_UNFUSED");
     p->fused = !(fz && fz[0] == '1');
     cudaGetDevice(&p->device);
-    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        set_global_error(WFD_ERR_CUDA, "stream creation failed");
-        delete p;
-        return nullptr;
-    }
-    p->own_stream = true;
+    // the arrays first, then the stream (an allocation failure is reported before any other call)
     const size_t bytes = sizeof(float) * (size_t)p->ncells();
     for (int f = 0; f < F_COUNT; f++) {
         if (!uses(phys, ndim, f)) continue;
-        cudaError_t e = cudaMallocManaged(&p->field[f], bytes, cudaMemAttachGlobal);
+        cudaError_t e = wfd::dMallocManaged(&p->field[f], bytes, cudaMemAttachGlobal);
         if (e != cudaSuccess) {
-            set_global_error(WFD_ERR_ALLOC, std::string("managed allocation failed: ") + cudaGetErrorString(e));
+            set_global_error(WFD_ERR_ALLOC, std::string("managed allocation failed: ") + cudaGetErrorString(e) +
+                                                alloc_injected_note());
             prop_destroy(p);
             return nullptr;
         }
+    }
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_global_error(WFD_ERR_CUDA, "stream creation failed");
+        prop_destroy(p);
+        return nullptr;
+    }
+    p->own_stream = true;
+    for (int f = 0; f < F_COUNT; f++) {
+        if (!p->field[f]) continue;
 #if CUDART_VERSION >= 13000
         cudaMemLocation loc{cudaMemLocationTypeDevice, p->device};
         cudaMemAdvise(p->field[f], bytes, cudaMemAdviseSetPreferredLocation, loc);
@@ -189,6 +222,8 @@ void prop_destroy(Prop *p) {
         if (p->field[f]) cudaFree(p->field[f]);
     for (int i = 0; i < 12; i++)
         if (p->tmp[i]) cudaFree(p->tmp[i]);
+    for (int i = 0; i < 7; i++)
+        if (p->stage[i]) cudaFree(p->stage[i]);
     if (p->work) cudaFree(p->work);
     if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
     delete p;
@@ -260,7 +295,7 @@ void prop_setup_q(Prop *p, float freqQ, float qMin, float qInterior) {
     for (long k = 0; k < ns; k++) table[k] = (float)((double)(dt * 2) * PI * (double)freqQ / (double)qprof[k]);
     table[ns] = (float)((double)(dt * 2) * PI * (double)freqQ / (double)qInterior);
     float *dtable = nullptr;
-    if (check_cuda(p, cudaMallocAsync(&dtable, sizeof(float) * table.size(), p->stream), "q table")) return;
+    if (check_cuda(p, wfd::dMallocAsync(&dtable, sizeof(float) * table.size(), p->stream), "q table")) return;
     cudaMemcpyAsync(dtable, table.data(), sizeof(float) * table.size(), cudaMemcpyHostToDevice, p->stream);
     Grid g = p->grid();
     k_fill_q<<<(unsigned)((g.n + 255) / 256), 256, 0, p->stream>>>(g, ns, dtable, p->field[F_Q]);
@@ -280,7 +315,7 @@ int prop_sync(Prop *p) {
 int prop_step(Prop *p, bool linear, bool sync) {
     Grid g = p->grid();
     Fields F = p->fields();
-    bool done = false, illum_done = false;
+    bool done = false, illum_done = false, epi_done = false;
     p->inject_done = false;
     if (p->fused) {
         const int r = p->strict ? wfd_strict::fused_step(g, p->phys, linear, F, p->stream)
@@ -288,6 +323,7 @@ int prop_step(Prop *p, bool linear, bool sync) {
         done = (r & 1) != 0;
         illum_done = (r & 2) != 0;
         p->inject_done = (r & 4) != 0;
+        epi_done = (r & 8) != 0;
     }
     if (!done) {
         if (!ensure_scratch(p, p->phys == ISO ? 3 : 6)) return p->status;
@@ -302,14 +338,59 @@ int prop_step(Prop *p, bool linear, bool sync) {
     }
     // the illumination of pCur (read-only during the step) when the step kernel did not add it
     if (p->illum && !illum_done) illum_accumulate(p->illum, p->field[F_PCUR], p->ncells(), p->stream);
+    const bool epi_wanted = p->epi.born_dv || p->epi.img || p->epi.scale_space;
     p->step_kernels = (done ? 1 : 2) + (p->illum && !illum_done ? 1 : 0);
     if (int rc = check_cuda(p, cudaGetLastError(), "time step launch")) return rc;
     // pointer swap (prop3DAcoIsoDenQ_DEO2_FDTD.h:258-260)
     std::swap(p->field[F_PCUR], p->field[F_POLD]);
     std::swap(p->field[F_MCUR], p->field[F_MOLD]);
     p->steps++;
+    if (epi_wanted && !epi_done) {
+        // the step kernel did not apply them: the separate kernels on the swapped fields (the new
+        // field is pCur, the step's input is pOld), as the reference's calls after TimeStep
+        Fields Fs = p->fields();
+        const StepEpilogue &e = p->epi;
+        const bool iso = p->phys == ISO;
+        if (e.scale_space) {
+            if (p->strict) wfd_strict::scale(g, Fs, !iso, p->stream);
+            else wfd_fast::scale(g, Fs, !iso, p->stream);
+            p->step_kernels++;
+        }
+        if (e.born_dv) {
+            if (iso) {
+                const float *lap[3] = {nullptr, nullptr, nullptr};
+                if (p->strict) wfd_strict::born_iso(g, 0, Fs, e.born_dv, nullptr, e.born_dp, lap, p->stream);
+                else wfd_fast::born_iso(g, 0, Fs, e.born_dv, nullptr, e.born_dp, lap, p->stream);
+            } else if (p->strict) {
+                wfd_strict::born_aniso_v(g, Fs, e.born_dv, e.born_dp, e.born_dm, p->stream);
+            } else {
+                wfd_fast::born_aniso_v(g, Fs, e.born_dv, e.born_dp, e.born_dm, p->stream);
+            }
+            p->step_kernels++;
+        }
+        if (e.img) {
+            if (iso) {
+                const float *t[3] = {nullptr, nullptr, nullptr};
+                if (p->strict) wfd_strict::image_iso(g, 0, Fs, e.img_dp, t, t, e.img, nullptr, p->stream);
+                else wfd_fast::image_iso(g, 0, Fs, e.img_dp, t, t, e.img, nullptr, p->stream);
+            } else if (p->strict) {
+                wfd_strict::image_aniso_v(g, Fs, e.img_dp, e.img_dm, e.img, p->stream);
+            } else {
+                wfd_fast::image_aniso_v(g, Fs, e.img_dp, e.img_dm, e.img, p->stream);
+            }
+            p->step_kernels++;
+        }
+        if (int rc = check_cuda(p, cudaGetLastError(), "Born/imaging launch")) return rc;
+    }
     if (sync) return prop_sync(p);
     return WFD_OK;
+}
+
+int prop_step_epilogue(Prop *p, const StepEpilogue &e, bool linear) {
+    p->epi = e;
+    const int rc = prop_step(p, linear, false);
+    p->epi = StepEpilogue{};
+    return rc;
 }
 
 int prop_scale(Prop *p) {

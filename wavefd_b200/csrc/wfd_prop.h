@@ -32,6 +32,7 @@ struct Prop {
     bool fused = true;       // single-sweep kernels where available
     float *field[F_COUNT] = {};
     float *tmp[12] = {};     // scratch of the unfused passes (the reference's tmp arrays)
+    float *stage[7] = {};    // device copies of host arrays given to Born/imaging calls (first use)
     float2 *work = nullptr;  // FFT workspace of the wavefield-separation condition
     float *illum = nullptr;  // caller's source illumination sum (device), accumulated by every step
     long work_cols = 0;
@@ -39,7 +40,9 @@ struct Prop {
     std::string message;
     long steps = 0;
     int step_kernels = 0;  // kernels launched by the last time step (1 fused, 2 unfused)
+    long run_launches = 0; // kernels launched by the last WFD_Prop_Run
     StepInject inj{};      // a source injection for the step kernel to apply (WFD_Prop_Run), or none
+    StepEpilogue epi{};    // Born injection / imaging condition to apply right after the next step, or none
     bool inject_done = false;  // the last step kernel applied `inj`
 
     long ncells() const { return nx * ny * nz; }
@@ -53,6 +56,9 @@ Prop *prop_create(int ndim, int phys, long fs, long nthread, long nx, long ny, l
 void prop_destroy(Prop *p);
 void prop_setup_q(Prop *p, float freqQ, float qMin, float qInterior);
 int prop_step(Prop *p, bool linear, bool sync);
+// one step followed by ForwardBornInjection_V (e.born_*) or AdjointBornAccumulation_V (e.img*), fused
+// into the step kernel where it can apply them, else as the separate kernels after it; asynchronous
+int prop_step_epilogue(Prop *p, const StepEpilogue &e, bool linear);
 int prop_scale(Prop *p);
 int prop_born(Prop *p, const char *variant, float *const *args, int nargs);
 int prop_image(Prop *p, const char *variant, float *const *args, int nargs, long isfwi);

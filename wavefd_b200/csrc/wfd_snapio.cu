@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_prop.h"
 
 namespace wfd {
@@ -386,7 +387,7 @@ extern "C" void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, i
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->copy, cudaStreamNonBlocking);
         for (auto &s : f->stage) {
             if (e == cudaSuccess) e = cudaHostAlloc(&s.host, (size_t)f->slot, cudaHostAllocDefault);
-            if (e == cudaSuccess) e = cudaMalloc(&s.dev, (size_t)f->slot);
+            if (e == cudaSuccess) e = wfd::dMalloc(&s.dev, (size_t)f->slot);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.host_ev, cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.dev_free_ev, cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming);

@@ -14,10 +14,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "wavefd_b200.h"
+#include "wfd_alloc.h"
 #include "wfd_points.h"
 #include "wfd_prop.h"
 
@@ -28,10 +31,10 @@ namespace {
 template <class T>
 bool upload(Table<T> &t, cudaStream_t s) {
     const size_t ng = (size_t)t.ngroups, np = (size_t)t.npoints;
-    if (cudaMallocAsync(&t.d_key, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
-    if (cudaMallocAsync(&t.d_start, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
-    if (cudaMallocAsync(&t.d_other, sizeof(long) * (np + 1), s) != cudaSuccess) return false;
-    if (cudaMallocAsync(&t.d_c, sizeof(T) * (np + 1), s) != cudaSuccess) return false;
+    if (wfd::dMallocAsync(&t.d_key, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
+    if (wfd::dMallocAsync(&t.d_start, sizeof(long) * (ng + 1), s) != cudaSuccess) return false;
+    if (wfd::dMallocAsync(&t.d_other, sizeof(long) * (np + 1), s) != cudaSuccess) return false;
+    if (wfd::dMallocAsync(&t.d_c, sizeof(T) * (np + 1), s) != cudaSuccess) return false;
     if (ng) cudaMemcpyAsync(t.d_key, t.key.data(), sizeof(long) * ng, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(t.d_start, t.start.data(), sizeof(long) * (ng + 1), cudaMemcpyHostToDevice, s);
     if (np) cudaMemcpyAsync(t.d_other, t.other.data(), sizeof(long) * np, cudaMemcpyHostToDevice, s);
@@ -117,20 +120,6 @@ __global__ void k_extract_tick(long ngroups, const long *__restrict__ key, const
     }
 }
 
-template <class T>
-__global__ void k_gather(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
-                         T *dst) {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[idx[i] * stride + off];
-}
-
-template <class T>
-__global__ void k_scatter(long n, const long *__restrict__ idx, long stride, long off, const T *__restrict__ src,
-                          T *dst) {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[idx[i] * stride + off] = src[i];
-}
-
 inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
 
 template <class T>
@@ -152,61 +141,146 @@ cudaStream_t st_stream() {
     return s;
 }
 
+// Drop-in tables are kept between calls: a time loop calls injectdata/extractdata every step with
+// the same partitions, and grouping, sorting and uploading 65,536 receivers every step would cost
+// more than the step. An entry is reused when the caller's partitions hold the same points (iu, ir
+// and the bits of c compared one by one, so a caller that rewrites its arrays in place gets a new
+// table); up to kCacheEntries tables stay resident, least recently used evicted first. Each entry
+// also keeps its device and pinned staging buffers. Calls are synchronous and serialised by the
+// cache lock, as the reference's calls are synchronous.
+constexpr int kCacheEntries = 8;
+
+template <class T>
+struct CachedTable {
+    Table<T> t;
+    int by_receiver = 0;
+    std::vector<PointsT<T>> raw;       // the caller's points, partition by partition
+    std::vector<long> counts;          // points per partition
+    unsigned long long last_use = 0;
+    T *d_dst = nullptr, *d_src = nullptr;  // device staging (groups, points)
+    T *h_dst = nullptr, *h_src = nullptr;  // pinned host staging
+};
+
+template <class T>
+bool same_points(const CachedTable<T> &e, int by_receiver, void **partitions, size_t npartitions,
+                 const long *npoints) {
+    if (e.by_receiver != by_receiver || e.counts.size() != npartitions) return false;
+    size_t j = 0;
+    for (size_t i = 0; i < npartitions; i++) {
+        if (e.counts[i] != npoints[i]) return false;
+        const PointsT<T> *p = reinterpret_cast<const PointsT<T> *>(partitions[i]);
+        for (long k = 0; k < npoints[i]; k++, j++) {
+            const PointsT<T> &q = e.raw[j];
+            if (p[k].iu != q.iu || p[k].ir != q.ir || memcmp(&p[k].c, &q.c, sizeof(T)) != 0) return false;
+        }
+    }
+    return true;
+}
+
+template <class T>
+void free_entry(CachedTable<T> *e, cudaStream_t s) {
+    release(e->t, s);
+    if (e->d_dst) cudaFreeAsync(e->d_dst, s);
+    if (e->d_src) cudaFreeAsync(e->d_src, s);
+    cudaStreamSynchronize(s);
+    if (e->h_dst) cudaFreeHost(e->h_dst);
+    if (e->h_src) cudaFreeHost(e->h_src);
+    delete e;
+}
+
+template <class T>
+struct TableCache {
+    std::mutex mu;
+    std::vector<CachedTable<T> *> entries;
+    unsigned long long clock = 0;
+};
+
+template <class T>
+TableCache<T> &table_cache() {
+    static TableCache<T> *c = new TableCache<T>();  // never destroyed: no CUDA calls at process exit
+    return *c;
+}
+
+// the entry for these partitions (built and uploaded on a miss), or nullptr on allocation failure
+template <class T>
+CachedTable<T> *lookup(TableCache<T> &cache, int by_receiver, void **partitions, size_t npartitions,
+                       const long *npoints, cudaStream_t s) {
+    for (CachedTable<T> *e : cache.entries)
+        if (same_points(*e, by_receiver, partitions, npartitions, npoints)) {
+            e->last_use = ++cache.clock;
+            return e;
+        }
+    CachedTable<T> *e = new CachedTable<T>();
+    e->by_receiver = by_receiver;
+    e->raw = flatten<T>(partitions, npartitions, npoints);
+    e->counts.assign(npoints, npoints + npartitions);
+    build(e->t, e->raw, by_receiver);
+    const size_t ng = (size_t)e->t.ngroups, np = (size_t)e->t.npoints;
+    bool ok = upload(e->t, s);
+    ok = ok && wfd::dMallocAsync(&e->d_dst, sizeof(T) * (ng + 1), s) == cudaSuccess;
+    ok = ok && wfd::dMallocAsync(&e->d_src, sizeof(T) * (np + 1), s) == cudaSuccess;
+    ok = ok && wfd::dMallocHost(&e->h_dst, sizeof(T) * (ng + 1)) == cudaSuccess;
+    ok = ok && wfd::dMallocHost(&e->h_src, sizeof(T) * (np + 1)) == cudaSuccess;
+    if (!ok) {
+        free_entry(e, s);
+        return nullptr;
+    }
+    if ((int)cache.entries.size() >= kCacheEntries) {
+        auto lru = std::min_element(cache.entries.begin(), cache.entries.end(),
+                                    [](const CachedTable<T> *a, const CachedTable<T> *b) {
+                                        return a->last_use < b->last_use;
+                                    });
+        free_entry(*lru, s);
+        cache.entries.erase(lru);
+    }
+    e->last_use = ++cache.clock;
+    cache.entries.push_back(e);
+    return e;
+}
+
 // Drop-in inject (by_receiver = 0) / extract (1). dst is written at key*dst_stride + dst_off,
-// src is read at other*src_stride + src_off.
+// src is read at other*src_stride + src_off. Device (or managed) arrays are read and written in
+// place by one kernel; host arrays go through the entry's pinned staging (the values the points
+// read, and the current values of the locations they write, up; the new values back).
 template <class T>
 void dropin(int by_receiver, T *dst, long dst_stride, long dst_off, const T *src, long src_stride, long src_off,
             void **partitions, size_t npartitions, const long *npoints) {
-    std::vector<PointsT<T>> pts = flatten<T>(partitions, npartitions, npoints);
-    if (pts.empty()) return;
+    long total = 0;
+    for (size_t i = 0; i < npartitions; i++) total += npoints[i];
+    if (total <= 0) return;
     cudaStream_t s = st_stream();
-    Table<T> t;
-    build(t, pts, by_receiver);
-    if (!upload(t, s)) {
+    TableCache<T> &cache = table_cache<T>();
+    std::lock_guard<std::mutex> lk(cache.mu);
+    CachedTable<T> *e = lookup(cache, by_receiver, partitions, npartitions, npoints, s);
+    if (!e) {
         set_global_error(WFD_ERR_ALLOC, "point table allocation failed");
-        release(t, s);
         return;
     }
+    const Table<T> &t = e->t;
     const bool dst_dev = device_accessible(dst);
     const bool src_dev = device_accessible(src);
     const long ng = t.ngroups, np = t.npoints;
-    T *d_dst = nullptr, *d_src = nullptr;
-    cudaMallocAsync(&d_dst, sizeof(T) * (size_t)ng, s);
-    // current values of the written locations
-    if (dst_dev) {
-        k_gather<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, dst_stride, dst_off, dst, d_dst);
-    } else {
-        std::vector<T> h((size_t)ng);
-        for (long g = 0; g < ng; g++) h[g] = dst[t.key[g] * dst_stride + dst_off];
-        cudaMemcpyAsync(d_dst, h.data(), sizeof(T) * (size_t)ng, cudaMemcpyHostToDevice, s);
-        cudaStreamSynchronize(s);
+    if (!src_dev) {
+        for (long j = 0; j < np; j++) e->h_src[j] = src[t.other[j] * src_stride + src_off];
+        cudaMemcpyAsync(e->d_src, e->h_src, sizeof(T) * (size_t)np, cudaMemcpyHostToDevice, s);
     }
-    // values read by every point
-    cudaMallocAsync(&d_src, sizeof(T) * (size_t)np, s);
-    std::vector<T> hs;
-    if (src_dev) {
-        k_gather<T><<<nb(np), 256, 0, s>>>(np, t.d_other, src_stride, src_off, src, d_src);
-    } else {
-        hs.resize((size_t)np);
-        for (long j = 0; j < np; j++) hs[j] = src[t.other[j] * src_stride + src_off];
-        cudaMemcpyAsync(d_src, hs.data(), sizeof(T) * (size_t)np, cudaMemcpyHostToDevice, s);
+    if (!dst_dev) {
+        for (long g = 0; g < ng; g++) e->h_dst[g] = dst[t.key[g] * dst_stride + dst_off];
+        cudaMemcpyAsync(e->d_dst, e->h_dst, sizeof(T) * (size_t)ng, cudaMemcpyHostToDevice, s);
     }
-    k_scatter_groups<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, t.d_start, t.d_other, t.d_c, d_dst, 0, 0, 1, d_src, 0,
-                                               0, 1);
-    if (dst_dev) {
-        k_scatter<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, dst_stride, dst_off, d_dst, dst);
-        cudaStreamSynchronize(s);
-    } else {
-        std::vector<T> h((size_t)ng);
-        cudaMemcpyAsync(h.data(), d_dst, sizeof(T) * (size_t)ng, cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        for (long g = 0; g < ng; g++) dst[t.key[g] * dst_stride + dst_off] = h[g];
+    k_scatter_groups<T><<<nb(ng), 256, 0, s>>>(ng, t.d_key, t.d_start, t.d_other, t.d_c,
+                                               dst_dev ? dst : e->d_dst, dst_dev ? dst_stride : 0,
+                                               dst_dev ? dst_off : 0, dst_dev ? 0 : 1,
+                                               src_dev ? src : e->d_src, src_dev ? src_stride : 0,
+                                               src_dev ? src_off : 0, src_dev ? 0 : 1);
+    if (!dst_dev) cudaMemcpyAsync(e->h_dst, e->d_dst, sizeof(T) * (size_t)ng, cudaMemcpyDeviceToHost, s);
+    cudaError_t err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) {
+        set_global_error(WFD_ERR_CUDA, cudaGetErrorString(err));
+        return;
     }
-    cudaFreeAsync(d_dst, s);
-    cudaFreeAsync(d_src, s);
-    release(t, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) set_global_error(WFD_ERR_CUDA, cudaGetErrorString(e));
+    if (!dst_dev)
+        for (long g = 0; g < ng; g++) dst[t.key[g] * dst_stride + dst_off] = e->h_dst[g];
 }
 
 struct DeviceTable {
@@ -254,7 +328,13 @@ extern "C" void *WFD_Points_Create(const SourcePoint32 *points, long npoints, in
         return nullptr;
     }
     std::vector<wfd::PointsT<float>> pts((size_t)npoints);
-    for (long i = 0; i < npoints; i++) pts[i] = {points[i].iu, points[i].ir, points[i].c};
+    for (long i = 0; i < npoints; i++) {
+        if (points[i].iu < 1 || points[i].ir < 1) {  // 1-based indices (spacetime.jl:793-797)
+            wfd::set_global_error(WFD_ERR_ARG, "WFD_Points_Create: indices are 1-based");
+            return nullptr;
+        }
+        pts[i] = {points[i].iu, points[i].ir, points[i].c};
+    }
     DeviceTable *d = new DeviceTable();
     wfd::build(d->t, pts, by_receiver);
     cudaStream_t s = wfd::st_stream();
@@ -349,12 +429,46 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     if (!p->fused || p->ndim == 2 || p->nz % 4 != 0)
         if (!wfd::ensure_scratch(p, p->phys == wfd::ISO ? 3 : 6)) return p->status;
     long *d_it = nullptr;
-    // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch
-    if (cudaMallocAsync(&d_it, 2 * sizeof(long), s) != cudaSuccess)
+    // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch;
+    // d_it[2..3]: the barrier words of the persistent 2D loop (count, generation, status)
+    if (wfd::dMallocAsync(&d_it, 4 * sizeof(long), s) != cudaSuccess)
         return wfd::prop_fail(p, WFD_ERR_ALLOC, "time index allocation failed");
-    const long init[2] = {it0, 0};
+    const long init[4] = {it0, 0, 0, 0};
     cudaMemcpyAsync(d_it, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
+    // 2D Iso: the whole loop in one cooperative launch (grid-wide barrier between steps)
+    if (p->ndim == 2 && p->phys == wfd::ISO && p->fused && !p->illum && nsteps > 0 &&
+        (!src || src->t.ngroups <= 1024)) {
+        wfd::Fields F = p->fields();
+        F.inj = wfd::StepInject{};
+        if (src && src->t.ngroups)
+            F.inj = wfd::StepInject{src->t.ngroups, src->t.d_key, src->t.d_start, src->t.d_other, src->t.d_c,
+                                    wavelet, nt, d_it};
+        wfd::RunExtract ex{};
+        if (rec && rec->t.ngroups)
+            ex = wfd::RunExtract{rec->t.ngroups, rec->t.d_key, rec->t.d_start, rec->t.d_other, rec->t.d_c, traces, nt};
+        unsigned *words = reinterpret_cast<unsigned *>(d_it + 2);
+        const wfd::Grid g = p->grid();
+        const int r = p->strict ? wfd_strict::iso2d_run(g, F, nsteps, it0, ex, words, s)
+                                : wfd_fast::iso2d_run(g, F, nsteps, it0, ex, words, s);
+        if (r == 0) {
+            unsigned status = 0;
+            cudaMemcpyAsync(&status, words + 2, sizeof status, cudaMemcpyDeviceToHost, s);
+            const cudaError_t e = cudaStreamSynchronize(s);
+            cudaFreeAsync(d_it, s);
+            if (e != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, std::string("time loop: ") + cudaGetErrorString(e));
+            if (status) return wfd::prop_fail(p, WFD_ERR_TIMEOUT, "time loop: a grid-wide barrier timed out");
+            if (nsteps & 1) std::swap(p->field[wfd::F_PCUR], p->field[wfd::F_POLD]);
+            p->steps += nsteps;
+            p->step_kernels = 1;
+            p->run_launches = 1;
+            return WFD_OK;
+        }
+        if (r > 0) {
+            cudaFreeAsync(d_it, s);
+            return wfd::prop_fail(p, WFD_ERR_CUDA, "time loop: cooperative launch failed");
+        }
+    }
     // a step kernel that can apply the injection itself (the 2D Iso kernel) gets the source table;
     // the per-CTA scan of the groups stays cheap for tables of up to 1024 groups
     p->inj = wfd::StepInject{};
@@ -390,6 +504,7 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
         }
     }
     for (; !rc && done < nsteps; done++) rc = run_step(p, src, wavelet, rec, traces, nt, d_it);
+    p->run_launches = nsteps * (long)p->step_kernels;
     p->inj = wfd::StepInject{};
     cudaFreeAsync(d_it, s);
     return rc;

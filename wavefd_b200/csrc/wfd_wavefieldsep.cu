@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "wfd_kernels.h"
+#include "wfd_alloc.h"
 
 namespace WFD_NS {
 using namespace wfd;
@@ -224,7 +225,7 @@ void image_wavefieldsep(const Grid &g, long isfwi, const Fields &F, const float 
             host_fft(vr, vi, -1);
             for (int j = 0; j < m; j++) h[(size_t)n + (size_t)sgn * m + j] = make_float2((float)vr[j], (float)vi[j]);
         }
-        cudaMallocAsync(&tables, sizeof(float2) * h.size(), s);
+        wfd::dMallocAsync(&tables, sizeof(float2) * h.size(), s);
         cudaMemcpyAsync(tables, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice, s);
         T.chirp = tables;
         T.vplus = tables + n;

@@ -5,7 +5,10 @@ This is the reference's workflow around the propagators (JetPackWaveFD drives Wa
 src/compressedio.jl:1-137 is its snapshot store): a forward run from the source saves the scaled
 spatial-derivative fields (pSpace, mSpace after ScaleSpatialDerivatives) every `every` steps; an
 adjoint run from the receivers back-propagates the recorded data and, at each saved step,
-accumulates the standard imaging condition (AdjointBornAccumulation_V) with the saved fields.
+accumulates the standard imaging condition (AdjointBornAccumulation_V) with the saved fields. Both are
+fused into the step kernels: the forward steps that save a snapshot write pSpace/mSpace already
+scaled (WFD_Prop_TimeStepScaled), and the adjoint steps at saved time indices accumulate the image
+as they step (WFD_Prop_TimeStepImage).
 
 Snapshot stores:
   CodecStore   -- the learned codec (wfd_codec.cu), codes resident in device memory;
@@ -278,8 +281,6 @@ def born_image(shot, data, store, every=4, nt=None):
     tsrc = lib.WFD_Points_Create(shot["src"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["src"]), 0)
     tadj = lib.WFD_Points_Create(shot["rec"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["rec"]), 0)
     image = torch.zeros(shape, device="cuda")
-    mtype = getattr(props, adj.NAME + "_Model_V")()
-    ic = props.ImagingConditionStandard()
     fs = torch.cuda.ExternalStream(fwd.stream())
     as_ = torch.cuda.ExternalStream(adj.stream())
     f_space = [_field(fwd, "PSpace", shape)] + ([_field(fwd, "MSpace", shape)] if aniso else [])
@@ -287,28 +288,35 @@ def born_image(shot, data, store, every=4, nt=None):
     props.scale_spatial_derivatives(adj)  # the device call after the getters (moves the arrays once)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    linear = shot["physics"] == "vti"
+    fp, ap = ct.c_void_p(fwd.p), ct.c_void_p(adj.p)
     for it in range(1, nt + 1):
-        fwd.step_async(1)
+        if it % every == 0:
+            # TimeStep with ScaleSpatialDerivatives fused into the step kernel (3D)
+            _lib.check(lib.WFD_Prop_TimeStepScaled(fp), "scaled step", fwd.p)
+        else:
+            fwd.step_async(1)
         _lib.check(lib.WFD_Inject(tsrc, fcur.step(), ct.c_void_p(shot["wavelet"].data_ptr()), it, shot["nt"],
                                   ct.c_void_p(fwd.stream())), "inject")
         if it % every == 0:
-            props.scale_spatial_derivatives(fwd)
             store.put(it // every - 1, f_space, fs)
     fwd.synchronize()
     for it in range(nt, 0, -1):
-        # self-adjoint steps: TimeStep (Iso, TTI), TimeStepLinear (VTI), as propagateadjoint does
-        adj.step_async(1, linear=shot["physics"] == "vti")
-        _lib.check(lib.WFD_Inject(tadj, acur.step(), ct.c_void_p(data.data_ptr()), it, shot["nt"],
-                                  ct.c_void_p(adj.stream())), "inject adjoint")
+        # self-adjoint steps: TimeStep (Iso, TTI), TimeStepLinear (VTI), as propagateadjoint does; at a
+        # saved step the imaging condition (AdjointBornAccumulation_V, which reads the step's input
+        # fields) is fused into the step kernel
         if it % every == 0:
             k = it // every - 1
             f = store.get(k, as_)
-            wf = {"pspace": f[0]}
-            if aniso:
-                wf["mspace"] = f[1]
-            props.adjointBornAccumulation(adj, mtype, ic, {"v": image}, wf)
+            dm = ct.c_void_p(f[1].data_ptr()) if aniso else None
+            _lib.check(lib.WFD_Prop_TimeStepImage(ap, ct.c_void_p(image.data_ptr()), ct.c_void_p(f[0].data_ptr()),
+                                                  dm, int(linear)), "imaging step", adj.p)
             if hasattr(store, "release"):
                 store.release(k, as_)
+        else:
+            adj.step_async(1, linear=linear)
+        _lib.check(lib.WFD_Inject(tadj, acur.step(), ct.c_void_p(data.data_ptr()), it, shot["nt"],
+                                  ct.c_void_p(adj.stream())), "inject adjoint")
     adj.synchronize()
     torch.cuda.synchronize()
     secs = time.perf_counter() - t0
