@@ -15,11 +15,17 @@ oracle/_ref) on the host cores for the same workload and prints the same JSON li
 """
 from __future__ import annotations
 
+import os
+
+# The reference's benchmark binds its OpenMP threads (benchmark/README.md: OMP_PROC_BIND=close); set
+# before any library that starts an OpenMP runtime is loaded in this process.
+os.environ.setdefault("OMP_PROC_BIND", "close")
+os.environ.setdefault("OMP_PLACES", "cores")
+
 import argparse
 import ctypes
 import json
 import math
-import os
 import statistics
 import subprocess
 import sys
@@ -117,6 +123,16 @@ class ClockSampler:
                                           "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # nvidia-smi takes a moment to start: wait (at most 5 s) for its first sample, so that the
+        # samples cover the load that follows
+        t0 = time.perf_counter()
+        while self.proc and time.perf_counter() - t0 < 5.0:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
@@ -148,11 +164,9 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------------
-def run_ours(args, W):
+def _dist_env():
+    """(world, rank, local rank, torch.distributed or None); the process group is created once."""
     import torch
-
-    from wavefd_b200 import _lib, props, synthetic
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -162,7 +176,18 @@ def run_ours(args, W):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if not dist.is_initialized():
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def run_ours(args, W):
+    """One single-shot workload on this rank's GPU; returns the JSON line (dict) on rank 0."""
+    import torch
+
+    from wavefd_b200 import _lib, props, synthetic
+
+    world, rank, local, dist = _dist_env()
     lib = _lib.library()
     nx, ny, nz = W["shape"]
     ncells = nx * ny * nz
@@ -194,19 +219,18 @@ def run_ours(args, W):
     wav = torch.from_numpy(causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"])).cuda()
     nrec = len(rec)
     traces = torch.zeros(nrec * nt, device="cuda")
-    pcur_name = "PCur"
+    getp = getattr(prop.abi, "getPCur")
 
     def step(it):
         _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
-        pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+        pc = ctypes.c_void_p(ctypes.cast(getp(prop.p), ctypes.c_void_p).value)
         _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, sptr), "inject")
         _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(traces.data_ptr()), pc, it, nt, sptr), "extract")
 
     K, Wu = args.steps, args.warmup
     if W.get("ndim", 3) == 2:
         # a small grid is bound by launch latency: the whole time loop runs through WFD_Prop_Run
-        run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells, rank, world, dist)
-        return
+        return run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells, rank, world, dist)
     it = 0
     for _ in range(Wu):
         it = it % nt + 1
@@ -220,13 +244,23 @@ def run_ours(args, W):
     ev1 = torch.cuda.Event(enable_timing=True)
     kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     with ClockSampler(local) as clk:
+        # untimed load of about a second first, so that the clock samples (every 200 ms) cover the GPU
+        # under load; the samples end with the timed region
+        t_load = time.perf_counter()
+        nload = 0
+        while time.perf_counter() - t_load < 1.0:
+            it = it % nt + 1
+            step(it)
+            nload += 1
+            if nload % 50 == 0:
+                prop.synchronize()
         ev0.record(stream)
         for i in range(K):
             it = it % nt + 1
             kev[i][0].record(stream)
             _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
             kev[i][1].record(stream)
-            pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+            pc = ctypes.c_void_p(ctypes.cast(getp(prop.p), ctypes.c_void_p).value)
             _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, sptr), "inject")
             _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(traces.data_ptr()), pc, it, nt, sptr), "extract")
         ev1.record(stream)
@@ -255,7 +289,7 @@ def run_ours(args, W):
             it = it % nt + 1
             d_sample.copy_(h_wav[it - 1:it], non_blocking=True)
             _lib.check(lib.WFD_Prop_TimeStepAsync(prop.p, 1, 0), "step", prop.p)
-            pc = ctypes.c_void_p(ctypes.cast(getattr(prop.abi, "get" + pcur_name)(prop.p), ctypes.c_void_p).value)
+            pc = ctypes.c_void_p(ctypes.cast(getp(prop.p), ctypes.c_void_p).value)
             _lib.check(lib.WFD_Inject(tsrc, pc, ctypes.c_void_p(d_sample.data_ptr()), 1, 1, sptr), "inject")
             d_rec.zero_()
             _lib.check(lib.WFD_Extract(trec, ctypes.c_void_p(d_rec.data_ptr()), pc, 1, 1, sptr), "extract")
@@ -267,6 +301,7 @@ def run_ours(args, W):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = float(t.item())
     e2e = world * ncells * K / t_e2e / 1e6
+    dropin = _dropin_loop(args, W, lib, prop, src, rec, nt, ncells, world, dist)
     # -- roofline of the step kernel(s) --------------------------------------------------------------
     kern_ms = statistics.mean(kms)
     alg_bytes = W["bytes_per_cell"] * ncells
@@ -275,6 +310,7 @@ def run_ours(args, W):
     traffic = profiled_traffic(W["name"])
     launches_per_step = lib.WFD_Prop_StepKernels(prop.p)
     clocks = clk.summary()
+    clocks["window"] = f"{nload} untimed steps (about 1 s) then the {K} timed steps"
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "Mcells/s", "n_gpus": world, "steps": K, "warmup": Wu,
         "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -285,6 +321,7 @@ def run_ours(args, W):
                           f"L2-resident by nature ({ncells * 4 / 1e6:.1f} MB per field), not flushed"),
                    "parallelism": f"shots x{world}"},
         "e2e": {"value": round(e2e, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * nrec},
+        "e2e_dropin": dropin,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "step kernel(s) of " + W["name"], "algorithmic_bytes_per_cell": W["bytes_per_cell"],
@@ -303,9 +340,56 @@ def run_ours(args, W):
         out["cpu_baseline"] = cpu_baseline(W)
     if dist:
         dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(out), flush=True)
+    return out if rank == 0 else None
+
+
+def _dropin_loop(args, W, lib, prop, src, rec, nt, ncells, world, dist):
+    """The reference's own call sequence (src/spacetime.jl:1157-1199 around propagateforward!):
+    TimeStep, injectdata_float and extractdata_float with host partitions (source_blocking /
+    receiver_blocking), a host wavelet and a host trace array, timed end to end on the host clock."""
+    import torch
+
+    from wavefd_b200.abi import SpacetimeABI
+    from wavefd_b200.spacetime import _partition_args, causal_ricker, receiver_blocking, source_blocking
+    st = SpacetimeABI(lib)
+    sb, rb = source_blocking(src, 8), receiver_blocking(rec, 8)
+    sp, sc = _partition_args(sb)
+    rp, rc = _partition_args(rb)
+    wav = causal_ricker(W["dt"] * np.arange(nt), f=W["fpeak"]).astype(np.float32)
+    traces = np.zeros(len(rec) * nt, np.float32)
+    fp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    step = getattr(prop.abi, "TimeStep")
+    getp = getattr(prop.abi, "getPCur")
+    it = 0
+
+    def one():
+        nonlocal it
+        it = it % nt + 1
+        step(prop.p)
+        pc = getp(prop.p)
+        st.injectdata_float(pc, fp(wav), it, nt, sp, len(sb), sc, 8)
+        st.extractdata_float(fp(traces), pc, rp, len(rb), rc, it, nt, 8)
+
+    for _ in range(3):
+        one()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    K = args.steps
+    t0 = time.perf_counter()
+    for _ in range(K):
+        one()
+    t = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return {"value": round(world * ncells * K / t / 1e6, 1), "unit": "Mcells/s", "steps": K,
+            "calls": "TimeStep + injectdata_float + extractdata_float (host wavelet, host traces, host partitions), "
+                     "synchronous as in the reference",
+            # injection reads the step's wavelet sample of every source point; extraction reads and writes
+            # back the step's sample of every receiver trace
+            "h2d_bytes_per_step": 4 * (len(src) + len(rec)), "d2h_bytes_per_step": 4 * len(rec)}
 
 
 def run_codec(args, W):
@@ -391,7 +475,8 @@ def run_born(args, W):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     _lib.library()
     every = W["every"]
-    ns = max(every, (args.steps // every) * every)
+    ns = max(every, (args.steps // every) * every)  # learned store: this many steps (3000 = the whole record)
+    ns_plain = min(ns, 200)  # plain pinned-host store: a sample (a whole shot's 629 GB exceeds host memory)
     codec = WavefieldCodec(seed=1)
     t0 = time.perf_counter()
     hist, nblocks = train_on_propagated(codec)
@@ -399,19 +484,21 @@ def run_born(args, W):
     shot = imaging.make_shot("tti", W["shape"], seed=4, d=W["d"], dt=W["dt"], nsponge=W["nsponge"], fpeak=W["fpeak"],
                              nt=ns, nrec=W["nrec"])
     data = imaging.born_data(shot)
-    nsnap = ns // every
     # warm-up (first launches, tensor maps, allocator)
     warm = dict(shot, nt=min(ns, 2 * every))
     imaging.born_image(warm, data, imaging.DeviceStore(W["shape"], 2, 2), every=every, nt=2 * every)
-    plain = imaging.HostStore(W["shape"], nsnap, 2)
     with ClockSampler(0) as clk:
-        img_plain, t_plain = imaging.born_image(shot, data, plain, every=every)
-        learned = imaging.CodecStore(codec, W["shape"], nsnap, 2)
+        plain = imaging.HostStore(W["shape"], ns_plain // every, 2)
+        img_plain, t_plain_sample = imaging.born_image(shot, data, plain, every=every, nt=ns_plain)
+        del plain
+        learned = imaging.CodecStore(codec, W["shape"], ns // every, 2)
         img_codec, t_codec = imaging.born_image(shot, data, learned, every=every)
+    t_plain = t_plain_sample * ns / ns_plain  # the plain store's cost per step is the same at every step
     # plain storage in a snapshot file on local disk (O_DIRECT), the fallback when 629 GB per shot fit
     # in neither device nor host memory: a shorter sample (at most 64 steps) so that it stays within
     # the box's disk and a couple of minutes
     disk = None
+    nsnap = ns // every
     disk_steps = min(ns, 64)
     disk_bytes = (disk_steps // every) * 2 * int(np.prod(W["shape"])) * 4
     tmpdir = os.environ.get("WFD_SNAP_DIR", tempfile.gettempdir())
@@ -426,6 +513,22 @@ def run_born(args, W):
                 "where": f"{tmpdir} (O_DIRECT where the file system allows)"}
     else:
         disk = {"unavailable": f"less than {1.5 * disk_bytes / 1e9:.0f} GB free in {tmpdir}"}
+    # image error at this shape: learned against exact FP32 snapshots kept in device memory, over as
+    # many steps (up to 600) as the device holds the exact snapshots for
+    import torch
+    snap_bytes = 2 * int(np.prod(W["shape"])) * 4
+    n_img = min(ns, 600)
+    free = torch.cuda.mem_get_info()[0]
+    while n_img > 4 * every and (n_img // every) * snap_bytes > 0.8 * free:
+        n_img -= 4 * every
+    exact_store = imaging.DeviceStore(W["shape"], n_img // every, 2)
+    img_e, _ = imaging.born_image(shot, data, exact_store, every=every, nt=n_img)
+    del exact_store
+    img_l, _ = imaging.born_image(shot, data, imaging.CodecStore(codec, W["shape"], n_img // every, 2), every=every,
+                                  nt=n_img)
+    ae, al = img_e.double(), img_l.double()
+    rel_full = float(torch.linalg.norm(al - ae) / torch.linalg.norm(ae).clamp_min(1e-30))
+    del img_e, img_l, ae, al
     # image error over a whole record (the sample's first steps image nothing yet): 128^3, 1000 steps
     small = imaging.make_shot("tti", (128, 128, 128), seed=4, d=W["d"], dt=W["dt"], nsponge=20, fpeak=W["fpeak"],
                               nt=1000, nrec=(32, 32))
@@ -434,7 +537,7 @@ def run_born(args, W):
     img_small, _ = imaging.born_image(small, sdata, imaging.CodecStore(codec, small["shape"], 250, 2), every=every)
     a, b = img_small.cpu().numpy().astype(np.float64), img_exact.cpu().numpy().astype(np.float64)
     rel = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
-    scale = W["nt"] / ns
+    scale = W["nt"] / ns  # 1 when the whole record was run
     ncells = int(np.prod(W["shape"]))
     out = {
         "metric": "Born image s/shot, learned compression vs plain storage (3D TTI DenQ)",
@@ -443,16 +546,21 @@ def run_born(args, W):
         "vs_baseline": None, "dtype": "f32 (codec: bf16 weights, fp32 accumulation)",
         "data": "synthetic (seeded TTI earth model, sparse +-2% reflectors on 20 horizons)",
         "config": {"workload": W["label"], "grid": list(W["shape"]), "time_steps_per_shot": W["nt"],
-                   "sample_steps": ns, "snapshot_every": every,
-                   "scaling_note": f"forward + adjoint of {ns} steps timed end to end, times {W['nt']}/{ns}"},
+                   "learned_steps": ns, "plain_host_steps": ns_plain, "snapshot_every": every,
+                   "scaling_note": (f"learned: forward + adjoint of {ns} steps timed end to end"
+                                    + (f", times {W['nt']}/{ns}" if ns != W["nt"] else " (the whole record)")
+                                    + f"; plain pinned-host: {ns_plain} steps, times {W['nt']}/{ns_plain}")},
         "plain_s_per_shot": round(t_plain * scale, 3),
         "speedup_learned_vs_plain": round(t_plain / t_codec, 3),
         "plain_disk": disk,
-        "plain_host_note": (f"pinned-host plain storage timed on the {ns}-step sample; a whole shot needs "
+        "plain_host_note": (f"pinned-host plain storage timed on a {ns_plain}-step sample; a whole shot needs "
                             f"{2 * ncells * 4 * (W['nt'] // every) / 1e9:.0f} GB of pinned host memory "
                             f"(this host: {_host_mem_gb():.0f} GB), so beyond the sample it is the disk store"),
         "image_rel_l2_learned_vs_plain": rel,
         "image_check": "TTI 128^3, nt 1000, snapshots every 4 steps, learned vs exact FP32 storage",
+        "image_rel_l2_at_bench_shape": rel_full,
+        "image_check_at_bench_shape": (f"TTI {'x'.join(map(str, W['shape']))}, the first {n_img} steps of the record "
+                                       f"imaged, learned vs exact FP32 snapshots in device memory"),
         "snapshot_bytes": {"plain": 2 * ncells * 4, "learned": 2 * codec.code_bytes(W["shape"])},
         "codec_training": {"seconds": round(t_train, 2), "blocks": nblocks, "steps": len(hist),
                            "final_loss": float(np.mean(hist[-50:]))},
@@ -640,6 +748,7 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
         ev1.record(stream)
         ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
+    timed_launches = int(lib.WFD_Prop_RunLaunches(prop.p))
     value = ncells * K / (ms / 1e3) / 1e6
     # end to end: chunks of C steps, wavelet chunk up, traces chunk down (pinned host memory)
     C = 100
@@ -669,7 +778,9 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
         "dtype": "f32", "data": "synthetic (seeded layered+random earth model, Gardner density, block Q)",
         "config": {"workload": W["label"], "grid": list(W["shape"]), "time_steps_per_shot": nt,
                    "l2": f"L2-resident by nature ({ncells * 4 / 1e6:.1f} MB per field), not flushed",
-                   "parallelism": f"shots x{world}", "time_loop": "CUDA graph of two steps (WFD_Prop_Run)"},
+                   "parallelism": f"shots x{world}",
+                   "time_loop": "WFD_Prop_Run: the whole loop in one cooperative launch (grid-wide barrier "
+                                "between steps)" if timed_launches == 1 else "WFD_Prop_Run: CUDA graph of two steps"},
         "e2e": {"value": round(ncells * K / t_e2e / 1e6, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 4 * nrec},
         "roofline": {"bound": "latency (L2-resident)", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -677,9 +788,9 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
                      "kernel": "whole step (kernels of " + W["name"] + " + injection + extraction)",
                      "algorithmic_bytes_per_cell": W["bytes_per_cell"], "kernel_ms": round(ms / K, 5),
                      "peak_source": peak_src},
-        # per step: the step kernel(s), the injection unless the step kernel applied it, the extraction
-        # with the time-index advance (WFD_Prop_StepKernels after WFD_Prop_Run)
-        "gpu_launches": K * lib.WFD_Prop_StepKernels(prop.p),
+        # kernels of the timed WFD_Prop_Run: one cooperative launch for the whole loop (2D Iso), else
+        # per step the step kernel(s), the injection unless the step kernel applied it, the extraction
+        "gpu_launches": timed_launches,
         "clocks": clk.summary(),
     }
     del traces, wav, d_wav, d_trc, h_trc, h_wav
@@ -687,10 +798,9 @@ def run_graph_2d(args, W, lib, prop, stream, tsrc, trec, wav, traces, nt, ncells
     lib.WFD_Points_Free(tsrc)
     lib.WFD_Points_Free(trec)
     props.free(prop)
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(W)
-    if rank == 0:
-        print(json.dumps(out), flush=True)
+    return out if rank == 0 else None
 
 
 def _managed_tensor(prop, getter, shape):
@@ -716,26 +826,57 @@ def _ref_flavour():
     return None
 
 
-def _cpu_run(W, nsteps_max, seconds, warmup=1, with_acq=True):
-    """Reference propagator on the host cores (oracle/_ref): returns (Mcells/s, steps, threads, flavour)."""
+def _physical_cores():
+    """Physical cores among the CPUs this process may run on (one OpenMP thread per core)."""
+    cpus = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
+    cores = set()
+    try:
+        phys = core = None
+        cpu = None
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "processor":
+                    cpu = int(v)
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and cpu is not None:
+                    if cpu in cpus:
+                        cores.add((phys, core) if core is not None else (None, cpu))
+                    cpu = phys = core = None
+        if cpu is not None and cpu in cpus:
+            cores.add((phys, core) if core is not None else (None, cpu))
+    except OSError:
+        pass
+    return max(1, len(cores) if cores else len(cpus))
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _ref_object(W, lib_name, fl, th, shape, nby, nbx):
     from oracle.oracle import reference_lib
-    from wavefd_b200.abi import PropagatorABI, SpacetimeABI
-    fl = _ref_flavour()
-    if fl is None:
-        return None
-    name = W["name"]
-    lib = reference_lib(name.replace("Prop", "prop"), fl)
-    abi = PropagatorABI(lib, name)
-    nx, ny, nz = W["shape"]
-    th = os.cpu_count() or 1
-    two = W.get("ndim", 3) == 2
-    if two:
-        p = abi.alloc(1, th, nx, nz, W["nsponge"], W["d"], W["d"], W["dt"], 8, nz)
+    from wavefd_b200.abi import PropagatorABI
+    lib = reference_lib(lib_name, fl)
+    abi = PropagatorABI(lib, W["name"])
+    nx, ny, nz = shape
+    if W.get("ndim", 3) == 2:
+        p = abi.alloc(1, th, nx, nz, W["nsponge"], W["d"], W["d"], W["dt"], nbx, nz)
     else:
-        p = abi.alloc(1, th, nx, ny, nz, W["nsponge"], W["d"], W["d"], W["d"], W["dt"], 8, 8, nz)
+        p = abi.alloc(1, th, nx, ny, nz, W["nsponge"], W["d"], W["d"], W["d"], W["dt"], nbx, nby, nz)
     abi.SetupDtOmegaInvQ(p, 5.0, 0.1, 100.0)
-    shp = (nx, ny, nz)
-    arr = lambda g: np.ctypeslib.as_array(getattr(abi, "get" + g)(p), shape=shp)
+    arr = lambda g: np.ctypeslib.as_array(getattr(abi, "get" + g)(p), shape=shape)
     arr("V")[...] = np.linspace(1500, 4500, nz, dtype=np.float32)[None, None, :]
     arr("B")[...] = 0.5
     if W["physics"] != "iso":
@@ -747,10 +888,64 @@ def _cpu_run(W, nsteps_max, seconds, warmup=1, with_acq=True):
             arr(g)[...] = v
     rng = np.random.default_rng(0)
     arr("PCur")[:, :, :64] = rng.standard_normal((nx, ny, min(64, nz))).astype(np.float32)[:, :, :64] * 1e-3
+    return abi, p, arr
+
+
+_TILE_CACHE = {}
+
+
+def _cpu_tile(W, fl, th):
+    """The reference's tile knobs for this grid on these cores: nbz = nz, and (nby, nbx) chosen like
+    its tilesize() (src/prop3DAcoIsoDenQ_DEO2_FDTD.jl:159-185, which times every pair of 4:2:64) on
+    the pairs {4, 8, 16, 32, 64}^2, each timed over 3 steps (median, after one) on a 32-plane slab of
+    the grid. Returns (nby, nbx, note)."""
+    key = (W["name"], tuple(W["shape"]), fl, th)
+    if key in _TILE_CACHE:
+        return _TILE_CACHE[key]
+    nx, ny, nz = W["shape"]
+    if W.get("ndim", 3) == 2:
+        cands = [(1, b) for b in (4, 8, 16, 32, 64)]
+    else:
+        cands = [(by, bx) for by in (4, 8, 16, 32, 64) for bx in (4, 8, 16, 32, 64)]
+    slab = (min(nx, 32), ny, nz)
+    best, rates = None, {}
+    for by, bx in cands:
+        abi, p, _ = _ref_object(W, W["name"].replace("Prop", "prop"), fl, th, slab, by, bx)
+        abi.TimeStep(p)
+        ts = []
+        for _ in range(3):
+            t1 = time.perf_counter()
+            abi.TimeStep(p)
+            ts.append(time.perf_counter() - t1)
+        abi.free(p)
+        rates[(by, bx)] = slab[0] * slab[1] * slab[2] / statistics.median(ts) / 1e6
+        if best is None or rates[(by, bx)] > rates[best]:
+            best = (by, bx)
+    note = (f"tiles nbz=nz, (nby, nbx) = {best} chosen from {{4,8,16,32,64}}^2 on a {slab[0]}-plane slab "
+            f"({rates[best]:.0f} Mcells/s there; (8, 8) gave {rates.get((8, 8), float('nan')):.0f})")
+    _TILE_CACHE[key] = (best[0], best[1], note)
+    return _TILE_CACHE[key]
+
+
+def _cpu_run(W, nsteps_max, seconds, warmup=1, with_acq=True):
+    """Reference propagator on the host cores (oracle/_ref): returns (Mcells/s, steps, threads, flavour,
+    step times, note). One OpenMP thread per physical core, bound close to cores (set at the top of
+    this file), tiles from _cpu_tile."""
+    fl = _ref_flavour()
+    if fl is None:
+        return None
+    from oracle.oracle import reference_lib
+    from wavefd_b200.abi import SpacetimeABI
+    name = W["name"]
+    nx, ny, nz = W["shape"]
+    th = _physical_cores()
+    two = W.get("ndim", 3) == 2
+    nby, nbx, tile_note = _cpu_tile(W, fl, th)
+    shp = (nx, ny, nz)
+    abi, p, arr = _ref_object(W, name.replace("Prop", "prop"), fl, th, shp, nby, nbx)
     st = None
     if with_acq:
         from wavefd_b200 import synthetic
-        from wavefd_b200.abi import SourcePoint32
         st = SpacetimeABI(reference_lib("spacetime", fl))
         if two:
             src, rec = synthetic.surface_acquisition_2d((nx, nz), W["d"])
@@ -787,7 +982,7 @@ def _cpu_run(W, nsteps_max, seconds, warmup=1, with_acq=True):
         times.append(time.perf_counter() - t1)
         n += 1
     abi.free(p)
-    return nx * ny * nz / statistics.median(times) / 1e6, n, th, fl, times
+    return nx * ny * nz / statistics.median(times) / 1e6, n, th, fl, times, tile_note
 
 
 def cpu_baseline(W):
@@ -795,11 +990,13 @@ def cpu_baseline(W):
     if r is None:
         return {"value": None, "unit": "Mcells/s", "cores": None, "kind": "reference",
                 "sample": "reference library not built"}
-    v, n, th, fl, _ = r
-    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+    v, n, th, fl, _, tile_note = r
+    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference", "cpu": _cpu_model(),
             "sample": f"{W['name']} TimeStep + injectdata_float + extractdata_float on the full "
                       f"{'x'.join(map(str, W['shape']))} grid, median of {n} steps after 1 warm-up, "
-                      f"{th} OpenMP threads, reference built with -O3 -ffast-math ({fl})"}
+                      f"{th} OpenMP threads (one per physical core, OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND')}, "
+                      f"OMP_PLACES={os.environ.get('OMP_PLACES')}), {tile_note}, reference built with "
+                      f"-O3 -ffast-math ({fl})"}
 
 
 def _batch_sample_ws(W, layout):
@@ -822,8 +1019,8 @@ def _batch_cpu_rate(W, layout, steps, warmup, seconds):
         r = _cpu_run(w, nsteps_max=steps, seconds=seconds, warmup=warmup)
         if r is None:
             return None
-        rates[ph], n, th, fl, _ = r
-        notes.append(f"{ph} {'x'.join(map(str, w['shape']))}: {rates[ph]:.1f} Mcells/s over {n} steps")
+        rates[ph], n, th, fl, _, tile_note = r
+        notes.append(f"{ph} {'x'.join(map(str, w['shape']))}: {rates[ph]:.1f} Mcells/s over {n} steps, {tile_note}")
     t = sum(nx * ny * nz / rates[ph] for ph, (nx, ny, nz), _ in layout)
     cells = sum(nx * ny * nz for _, (nx, ny, nz), _ in layout)
     return cells / t, th, fl, "; ".join(notes)
@@ -835,55 +1032,73 @@ def cpu_baseline_batch(W, layout):
         return {"value": None, "unit": "Mcells/s", "cores": None, "kind": "reference",
                 "sample": "reference library not built"}
     v, th, fl, notes = r
-    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
+    return {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference", "cpu": _cpu_model(),
             "sample": f"reference TimeStep + injectdata_float + extractdata_float on one mean-size Iso and one "
                       f"VTI window ({notes}), median step times, combined over the batch's 64 windows; "
-                      f"{th} OpenMP threads, -O3 -ffast-math ({fl})"}
+                      f"{th} OpenMP threads (one per physical core, bound close to cores), -O3 -ffast-math ({fl})"}
+
+
+def _unavailable(why):
+    return {"impl": "reference", "unavailable": why}
 
 
 def run_reference(args, W):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
+    """The reference's own C++/OpenMP implementation (oracle/_ref, compiled from its sources) on this
+    host's cores, same workload, metric and unit; returns the JSON line (rank 0 only)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
     if _ref_flavour() is None:
-        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (make -C oracle ref)"}))
-        return
+        return _unavailable("reference library not built (make -C oracle ref)")
     if W["name"] == "codec":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference compresses with CvxCompress, a Julia "
-                          "package absent from the reference tree and from this image"}))
-        return
+        return _unavailable("the reference compresses with CvxCompress, a Julia package absent from the "
+                            "reference tree and from this image")
     if W["name"] == "born":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's Born imaging stores its snapshots "
-                          "through CvxCompress (src/compressedio.jl), a Julia package absent here"}))
-        return
+        return _unavailable("the reference's Born imaging stores its snapshots through CvxCompress "
+                            "(src/compressedio.jl), a Julia package absent here")
     if W["name"] == "batch":
         layout = batch_layout(W)
         v, th, fl, notes = _batch_cpu_rate(W, layout, steps=args.steps, warmup=args.warmup, seconds=60.0)
         cells = sum(nx * ny * nz for _, (nx, ny, nz), _ in layout)
-        out = {
+        return {
             "metric": METRIC, "value": round(v, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(cells / v / 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": W["label"], "parallelism": f"OpenMP x{th}"},
             "cpu_baseline": {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
-                             "sample": notes},
+                             "cpu": _cpu_model(), "sample": notes},
             "e2e": {"value": round(v, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
-        print(json.dumps(out), flush=True)
-        return
     r = _cpu_run(W, nsteps_max=args.steps, seconds=1e9, warmup=args.warmup)
-    v, n, th, fl, times = r
+    v, n, th, fl, times, tile_note = r
     ms = statistics.mean(times) * 1e3
-    out = {
+    return {
         "metric": METRIC, "value": round(v, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": n, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "impl": "reference",
         "config": {"workload": W["label"], "grid": list(W["shape"]), "parallelism": f"OpenMP x{th}"},
         "cpu_baseline": {"value": round(v, 1), "unit": "Mcells/s", "cores": th, "kind": "reference",
-                         "sample": f"{n} full-grid steps (TimeStep + inject + extract), median"},
+                         "cpu": _cpu_model(),
+                         "sample": f"{n} full-grid steps (TimeStep + inject + extract), median; {th} OpenMP threads "
+                                   f"(one per physical core, bound close to cores); {tile_note}; -O3 -ffast-math "
+                                   f"({fl})"},
         "e2e": {"value": round(v, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(out), flush=True)
+
+
+# Secondary workloads timed in the same run as the headline one (same JSON line, key "legs"): the
+# 3D TTI step is the north-star kernel, timed on the 3D TTI workload's 400^3 grid.
+LEGS = {"iso512": ["tti400"]}
+
+
+def _relaunch_distributed(args):
+    """--gpus N without a launcher: run this script as N ranks (one per GPU) under torchrun."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -894,25 +1109,44 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="iso512", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="time the headline workload only")
     args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return _relaunch_distributed(args)
+    if world != args.gpus and args.impl == "ours":
+        raise SystemExit(f"--gpus {args.gpus} but this launch has {world} ranks")
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     W = WORKLOADS[args.workload]
+    legs = [] if args.no_legs else LEGS.get(args.workload, [])
     if args.impl == "reference":
-        run_reference(args, W)
+        out = run_reference(args, W)
+        if out is not None and "unavailable" not in out and legs:
+            out["legs"] = {k: run_reference(args, WORKLOADS[k]) for k in legs}
     elif W["name"] == "batch":
         run_batch(args, W)
+        return 0
     elif W["name"] == "born":
         run_born(args, W)
+        return 0
     elif W["name"] == "codec":
         run_codec(args, W)
+        return 0
     else:
-        run_ours(args, W)
-    # leave without running interpreter-teardown destructors (CUDA objects owned by two runtimes)
-    sys.stdout.flush()
-    sys.stderr.flush()
-    os._exit(0)
+        out = run_ours(args, W)
+        leg_out = {k: run_ours(args, WORKLOADS[k]) for k in legs}
+        if out is not None and legs:
+            out["legs"] = leg_out
+            out["gpu_launches"] += sum(v.get("gpu_launches", 0) for v in leg_out.values())
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

@@ -280,7 +280,7 @@ def test_prop_run_index_advance(lib, nrec):
         ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), 1, 0)
         tr = None
         if nrec:
-            rec = (SourcePoint32 * nrec)(*[SourcePoint32((7 * i) % ncell, i + 1, 1.0) for i in range(nrec)])
+            rec = (SourcePoint32 * nrec)(*[SourcePoint32((7 * i) % ncell + 1, i + 1, 1.0) for i in range(nrec)])
             tr = lib.WFD_Points_Create(ctypes.cast(rec, ctypes.POINTER(SourcePoint32)), nrec, 1)
         wav = torch.from_numpy(np.random.default_rng(2).standard_normal(nt).astype(np.float32)).cuda()
         trc = torch.zeros(max(nrec, 1) * nt, device="cuda")
