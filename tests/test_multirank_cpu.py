@@ -78,3 +78,46 @@ def test_two_gloo_ranks_reduce_images(tmp_path):
     got = np.load(out)
     want = sum(_shot_image(100 + s, shape) for s in range(nshots))
     assert np.allclose(got, want, rtol=1e-6, atol=1e-12)
+
+
+def _ledger_rank(rank, world, port, ledger_base, nshots, stop_after, out):
+    import torch.distributed as dist
+
+    from wavefd_b200.shots import ShotLedger, partition_shots
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    led = ShotLedger(ledger_base, rank)
+    todo = led.pending(partition_shots(nshots, world, rank))
+    ran = []
+    for s in todo:
+        if stop_after is not None and len(ran) == stop_after:
+            break  # the job stops here (a restart picks up the rest)
+        ran.append(s)
+        led.done(s)
+    with open(f"{out}.{rank}", "a") as f:
+        f.write(" ".join(map(str, ran)) + "\n")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_shot_ledger_resume_two_ranks(tmp_path):
+    """Two gloo ranks stop after one shot each; the restarted job runs only the remaining shots, and
+    every shot is run exactly once over both runs. A half-written line (a crash mid-write) is ignored."""
+    nshots = 7
+    base = str(tmp_path / "ledger")
+    out = str(tmp_path / "ran")
+    mp.start_processes(_ledger_rank, args=(2, _free_port(), base, nshots, 1, out), nprocs=2, join=True,
+                       start_method="spawn")
+    with open(base + ".rank1", "a") as f:
+        f.write("1 6")  # no newline: cut short
+    mp.start_processes(_ledger_rank, args=(2, _free_port(), base, nshots, None, out), nprocs=2, join=True,
+                       start_method="spawn")
+    ran = []
+    for r in range(2):
+        with open(f"{out}.{r}") as f:
+            for line in f:
+                ran += [int(x) for x in line.split()]
+    assert sorted(ran) == list(range(nshots))
+    from wavefd_b200.shots import ShotLedger
+    assert ShotLedger(base).finished() == set(range(nshots))

@@ -48,3 +48,54 @@ def reduce_image(image, dst: int = 0):
         return image
     dist.reduce(image, dst=dst, op=dist.ReduceOp.SUM)
     return image
+
+
+class ShotLedger:
+    """Shot-level resume: an append-only file of the shots whose results are saved.
+
+    The reference keeps no record of finished work (a run that stops is run again). Here each rank
+    records a shot after its contribution is safely stored (`done`, one line written and flushed to
+    disk per shot), and a restarted job asks for the shots still to do (`pending`). Lines are
+    "rank shot" text; a line cut short by a crash is ignored (and dropped when that rank's ledger is
+    opened again, before it appends). Ranks write to their own file
+    (path + ".rank<r>"), so no locking is needed; `pending` reads every rank's file.
+    """
+
+    def __init__(self, path: str, rank: int = 0):
+        import os
+        self.base = str(path)
+        self.rank = int(rank)
+        self.path = f"{self.base}.rank{self.rank}"
+        d = os.path.dirname(self.path)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        # a record cut short by a crash (no newline) is dropped before this rank appends again
+        if os.path.exists(self.path):
+            with open(self.path, "rb+") as f:
+                data = f.read()
+                if data and not data.endswith(b"\n"):
+                    f.truncate(data.rfind(b"\n") + 1)
+
+    def done(self, shot: int):
+        import os
+        with open(self.path, "a") as f:
+            f.write(f"{self.rank} {int(shot)}\n")
+            f.flush()
+            os.fsync(f.fileno())
+
+    def finished(self):
+        import glob
+        out = set()
+        for p in glob.glob(f"{self.base}.rank*"):
+            with open(p) as f:
+                for line in f:
+                    if not line.endswith("\n"):
+                        continue  # cut short
+                    parts = line.split()
+                    if len(parts) == 2 and parts[1].lstrip("-").isdigit():
+                        out.add(int(parts[1]))
+        return out
+
+    def pending(self, shots):
+        fin = self.finished()
+        return [s for s in shots if s not in fin]
