@@ -833,32 +833,27 @@ def _ref_flavour():
     return None
 
 
-def _physical_cores():
-    """Physical cores among the CPUs this process may run on (one OpenMP thread per core)."""
+def _count_physical_cores():
+    """Physical cores among the CPUs this process may run on: the distinct hyperthread-sibling sets of
+    those CPUs (sysfs topology), else the CPU count."""
     cpus = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
-    cores = set()
-    try:
-        phys = core = None
-        cpu = None
-        with open("/proc/cpuinfo") as f:
-            for line in f:
-                k, _, v = line.partition(":")
-                k, v = k.strip(), v.strip()
-                if k == "processor":
-                    cpu = int(v)
-                elif k == "physical id":
-                    phys = v
-                elif k == "core id":
-                    core = v
-                elif not k and cpu is not None:
-                    if cpu in cpus:
-                        cores.add((phys, core) if core is not None else (None, cpu))
-                    cpu = phys = core = None
-        if cpu is not None and cpu in cpus:
-            cores.add((phys, core) if core is not None else (None, cpu))
-    except OSError:
-        pass
-    return max(1, len(cores) if cores else len(cpus))
+    sets = set()
+    for c in cpus:
+        try:
+            with open(f"/sys/devices/system/cpu/cpu{c}/topology/thread_siblings_list") as f:
+                sets.add(f.read().strip())
+        except OSError:
+            return max(1, len(cpus))
+    return max(1, len(sets))
+
+
+# counted before any OpenMP runtime binds this process's main thread to one core (OMP_PROC_BIND
+# narrows the affinity that a later count would see)
+_PHYS_CORES = _count_physical_cores()
+
+
+def _physical_cores():
+    return _PHYS_CORES
 
 
 def _cpu_model():

@@ -26,11 +26,7 @@ int fused_step(const Grid &g, int phys, int linear, const Fields &F, cudaStream_
         if (fused_vti3d_tma(g, linear, Fe, s)) return 1 | lit | ept;
         return fused_aniso3d_tma(g, phys, linear, Fn, s) ? 1 : 0;
     }
-    if (g.ndim == 3 && phys == TTI) {
-        // the split-role kernel, else the ring kernel
-        if (!linear && fused_tti3d_split(g, Fe, s)) return 1 | lit | ept;
-        return fused_aniso3d_tma(g, phys, linear, Fl, s) ? 1 | lit : 0;
-    }
+    if (g.ndim == 3 && phys == TTI) return fused_aniso3d_tma(g, phys, linear, Fe, s) ? 1 | lit | ept : 0;
     if (g.ndim == 2 && phys == ISO) {
         Fields Fi = Fn;
         Fi.inj = F.inj;

@@ -25,8 +25,6 @@
 // columns of the top tile. With an illumination sum attached (single objects), each cell's pCur^2
 // is added to it as the cell is updated. Waits are bounded; on timeout the kernel records an error
 // in a device status word and leaves. Requires nz % 4 == 0 (TMA row pitch).
-#include <stdlib.h>
-
 #include "wfd_kernels.h"
 #include "wfd_tma.cuh"
 
@@ -275,7 +273,7 @@ __device__ __forceinline__ void queue_phase(const Grid &g, float2 (&qx)[8][2], f
 // BATCH = false: one propagator object, tensor maps in the kernel parameters, static items.
 // BATCH = true: many shots; each item names its shot, whose sizes, output pointers and tensor maps
 // sit in a descriptor in global memory; CTAs take items from a shared counter.
-template <int PHYS, bool LINEAR, bool BATCH>
+template <int PHYS, bool LINEAR, bool BATCH, bool EPI = false>
 __global__ void __launch_bounds__(NT, 1)
     k_aniso3d_tma(Grid g0, Fields F, const __grid_constant__ AnisoMaps M, int ntz0, int nty0, int nch0, int xchunk0,
                   const AnisoShotDesc *__restrict__ shots, const int *__restrict__ sel,
@@ -559,14 +557,34 @@ __global__ void __launch_bounds__(NT, 1)
                 const float2 k2 = div2(mul2(mul2(bc2(g.dt2), V), V), B);
                 const long k = j * g.sx + (long)y * g.nz + z;
                 const int ro = (row + 7) * RZW + 8 + 2 * zp;
+                // Born-V injection fused after the step (prop3DAcoTTIDenQ_DEO2_FDTD.h:423-452):
+                // new += 2 dt^2 dV/V * DP (DM), every cell
+                float2 bfac = bc2(0.0f);
+                if (EPI && F.epi.born_dv) bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), ld2(F.epi.born_dv + k)), V);
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
                     const float2 pc = ld2(ring[0] + f * RBOX + ro);
                     const float2 po = ld2(cs + (f == 0 ? C_PO : C_MO) * CBOX + o);
                     const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc, po))), po);
                     const float2 np = add2(t, mul2(bc2(2.0f), pc));
-                    st2((f == 0 ? out_pold : out_mold) + k, ok ? np : po);
-                    if (!LINEAR) st2((f == 0 ? out_pspace : out_mspace) + k, ok ? L[f] : bc2(0.0f));
+                    float2 nv = ok ? np : po;
+                    if (EPI && F.epi.born_dv) nv = add2(nv, mul2(bfac, ld2((f == 0 ? F.epi.born_dp : F.epi.born_dm) + k)));
+                    st2((f == 0 ? out_pold : out_mold) + k, nv);
+                    if (!LINEAR) {
+                        float2 sp = ok ? L[f] : bc2(0.0f);
+                        // ScaleSpatialDerivatives fused (.h:387-415): pSpace, mSpace *= V^2/B
+                        if (EPI && F.epi.scale_space) sp = mul2(sp, div2(mul2(V, V), B));
+                        st2((f == 0 ? out_pspace : out_mspace) + k, sp);
+                    }
+                }
+                if (EPI && F.epi.img) {
+                    // imaging condition fused after the step (.h:567-592): img += 2B/V^3 (DP pOld + DM
+                    // mOld), pOld/mOld being this step's input pCur/mCur
+                    const float2 pcp = ld2(ring[0] + ro), pcm = ld2(ring[0] + RBOX + ro);
+                    const float2 fac = div2(mul2(bc2(2.0f), B), mul2(mul2(V, V), V));
+                    float2 a = ld2(F.epi.img + k);
+                    a = add2(a, mul2(fac, add2(mul2(ld2(F.epi.img_dp + k), pcp), mul2(ld2(F.epi.img_dm + k), pcm))));
+                    st2(F.epi.img + k, a);
                 }
                 if (!BATCH && F.illum) {
                     // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add,
@@ -594,329 +612,6 @@ __global__ void __launch_bounds__(NT, 1)
     }
 }
 
-// ---- split-role TTI step -------------------------------------------------------------------------
-// The same arithmetic as k_aniso3d_tma<TTI>, with 512 threads in two roles so that twice as many
-// warps hide the latency of the dependent stencil chains: threads 0-255 ("tile") evaluate pass 1 on
-// the tile's pairs at the lead plane and pass 2 of the P field at plane j; threads 256-511 evaluate
-// pass 1 on the halo pairs (warps 8-11: the 7 extended rows of y outputs, 28 pairs a warp; warps
-// 12-13: the 8 extended columns of z outputs) and pass 2 of the M field at plane j for the tile
-// pair of the same index. The tile's M x output goes from one role to the other through shared
-// memory; the y/z outputs of the lead plane go to a 5-slot ring, read three iterations later.
-// Pass 2 reads its single-cell inputs (pOld or mOld, V, Q, b, pCur or mCur at plane j) from global
-// memory, so shared memory holds only the pCur/mCur ring (9 planes) and the material stages (2).
-// One barrier a plane: a slot is reused only after every thread has passed a later barrier.
-namespace split {
-constexpr int NT2 = 512;
-constexpr int NR2 = 9;   // ring planes: the 8 of the x window plus one in flight
-constexpr int NM2 = 2;   // material stages
-constexpr int NS2 = 5;   // y/z output slots: written at lead plane P, read at P-3, one iteration of slack
-constexpr int YZ = 2 * TYR * TZ + 2 * TY * TZW;  // floats per y/z slot: TY outputs [2][TYR][TZ], TZ [2][TY][TZW]
-constexpr int O_RING = 0;
-constexpr int O_MAT = O_RING + NR2 * R_SLOT;
-constexpr int MSTAGE = NMAT * MBOX;
-constexpr int O_YZ = O_MAT + NM2 * MSTAGE;
-constexpr int O_MX = O_YZ + NS2 * YZ;  // [2][256] float2: the tile's M x outputs
-constexpr int O_BAR = O_MX + 2 * 2 * 256;
-constexpr size_t SMEM2 = (size_t)O_BAR * 4 + (NR2 + NM2) * 8 + 16;
-constexpr int PRODUCER = 511;  // issues the copies: the last lane of warp 15 (no pass-1 work)
-static_assert((O_MAT * 4) % 128 == 0 && (MSTAGE * 4) % 128 == 0 && (R_SLOT * 4) % 128 == 0, "TMA alignment");
-static_assert(O_BAR % 2 == 0, "mbarrier alignment");
-static_assert(SMEM2 <= 232448, "shared memory per CTA");
-}  // namespace split
-
-__device__ __forceinline__ float2 ldg2(const float *p) { return __ldg(reinterpret_cast<const float2 *>(p)); }
-
-// x-output queue of one field: the output of the lead plane enters slot (PH+3)&7, and the D- x
-// stencil of plane j = P-3 runs over slots (PH+4)&7 .. (PH+3)&7 (planes j-4 .. j+3)
-template <int PH>
-__device__ __forceinline__ float2 xqueue(const Grid &g, float2 (&qx)[8], float2 in) {
-    qx[(PH + 3) & 7] = in;
-    return st8d(g, g.idx, qx[(PH + 4) & 7], qx[(PH + 5) & 7], qx[(PH + 6) & 7], qx[(PH + 7) & 7], qx[(PH + 0) & 7],
-                qx[(PH + 1) & 7], qx[(PH + 2) & 7], qx[(PH + 3) & 7]);
-}
-
-__global__ void __launch_bounds__(split::NT2, 1)
-    k_tti3d_split(Grid g, Fields F, const __grid_constant__ AnisoMaps M, int ntz, int nty, int nch, int xchunk) {
-    using namespace split;
-    extern __shared__ __align__(1024) float sm[];
-    uint64_t *rbar = reinterpret_cast<uint64_t *>(sm + O_BAR);
-    uint64_t *mbar = rbar + NR2;
-    // abort flags by iteration parity: set in pass 1 of an iteration, read after its barrier, not
-    // written again until every thread has passed the next barrier
-    int *abort2 = reinterpret_cast<int *>(mbar + NM2);
-    float *MX = sm + O_MX;
-    const int tid = threadIdx.x;
-    if (tid == 0) {
-        for (int i = 0; i < NR2; i++) mbar_init(&rbar[i], 1);
-        for (int i = 0; i < NM2; i++) mbar_init(&mbar[i], 1);
-        fence_mbar_init();
-        abort2[0] = abort2[1] = 0;
-    }
-    for (int i = tid; i < NS2 * YZ; i += NT2) sm[O_YZ + i] = 0.0f;
-    __syncthreads();
-
-    const bool tile_role = tid < 256;
-    const int u = tid & 255;  // tile pair of this thread's pass 2 (and pass 1 in the tile role)
-    const int zp = u & 15, row = u >> 4;
-    const int fld = tile_role ? 0 : 1;  // pass-2 field: P (tile role) or M
-    // pass-1 halo task of the other role: kind 1 = y outputs of an extended row, 2 = z outputs of an
-    // extended column pair, 0 = none
-    int h_kind = 0, h_er = 4, h_ec = 4, h_zp = 1;
-    if (!tile_role) {
-        if (u < 128) {
-            const int l = u & 31;
-            if (l < 28) {
-                const int t = (u >> 5) * 28 + l;  // 0..111: 7 rows x 16 pairs
-                const int hr = t >> 4;
-                h_er = hr < 4 ? hr : hr + 16;
-                h_zp = t & 15;
-                h_ec = 4 + 2 * h_zp;
-                h_kind = 1;
-            }
-        } else if (u < 192) {
-            const int v = u - 128;  // 0..63: 16 rows x 4 column pairs
-            const int hp = v & 3;
-            h_er = 4 + (v >> 2);
-            h_ec = hp < 2 ? 2 * hp : 36 + 2 * (hp - 2);
-            h_kind = 2;
-        }
-    }
-    const int img = tile_role ? -1 : u - 192;  // 0..45: writers of the free-surface image (2 fields x 23 rows)
-
-    const long total = (long)ntz * nty * nch;
-    unsigned rseq = 0, mseq = 0, sseq = 0;  // ring planes, material stages and iterations done by this CTA
-    unsigned r_issued = 0, m_issued = 0, r_done = 0, m_done = 0;
-    bool stop = false;
-    const CUtensorMap *mP = M.m + 0, *mM = M.m + 1, *mB = M.m + 2, *mE = M.m + 3, *mA = M.m + 4, *mF = M.m + 5,
-                      *mST = M.m + 6, *mCT = M.m + 7, *mSP = M.m + 8, *mCP = M.m + 9;
-    for (long w = blockIdx.x; w < total && !stop; w += gridDim.x) {
-        const int tzi = (int)(w % ntz);
-        const int tyi = (int)((w / ntz) % nty);
-        const int chi = (int)(w / ((long)ntz * nty));
-        const int z0 = tzi * TZ, y0 = tyi * TY;
-        const long xbeg = (long)chi * xchunk;
-        const long xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
-        const long jstart = xbeg - WARMUP;
-        const int niter = (int)(xend - jstart);
-        const int nplanes = niter + 7;  // ring planes jstart .. xend+6
-        const bool top = z0 == 0 && g.fs;
-        const int z = z0 + 2 * zp, y = y0 + row;
-        const bool own = z < g.nz && y < g.ny;
-        const int hz = z0 - 4 + h_ec, hy = y0 - 4 + h_er;
-        const bool yz_tile = yok(g, y) && zok(g, z), yz_halo = yok(g, hy) && zok(g, hz);
-
-        auto issue_ring = [&](int rp, unsigned gidx) {
-            uint64_t *bar = &rbar[gidx % NR2];
-            float *s = sm + O_RING + (gidx % NR2) * R_SLOT;
-            mbar_expect_tx(bar, 4u * R_SLOT);
-            tma_load_3d(s, mP, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
-            tma_load_3d(s + RBOX, mM, bar, z0 - 8, y0 - 7, (int)(jstart + rp));
-        };
-        auto issue_mat = [&](int q, unsigned gidx) {
-            uint64_t *bar = &mbar[gidx % NM2];
-            float *s = sm + O_MAT + (gidx % NM2) * MSTAGE;
-            mbar_expect_tx(bar, 4u * NMAT * MBOX);
-            const int P = (int)(jstart + q + 3);
-            tma_load_3d(s + MT_B * MBOX, mB, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_E * MBOX, mE, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_A * MBOX, mA, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_F * MBOX, mF, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_ST * MBOX, mST, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_CT * MBOX, mCT, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_SP * MBOX, mSP, bar, z0 - 4, y0 - 4, P);
-            tma_load_3d(s + MT_CP * MBOX, mCP, bar, z0 - 4, y0 - 4, P);
-        };
-        // antisymmetric image p[-k] = -p[k] (k = 1..3) above the free surface, in one ring plane
-        auto image_plane = [&](unsigned gidx) {
-            if (img >= 0 && img < 46) {
-                float *s = sm + O_RING + (gidx % NR2) * R_SLOT + (img / 23) * RBOX + (3 + img % 23) * RZW;
-                s[7] = -s[9];  // column of kz is kz + 8
-                s[6] = -s[10];
-                s[5] = -s[11];
-            }
-        };
-
-        if (tid == PRODUCER) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            const int nr0 = nplanes < NR2 ? nplanes : NR2;
-            for (int rp = 0; rp < nr0; rp++) issue_ring(rp, r_issued + rp);
-            r_issued += nr0;
-            const int nm0 = niter < NM2 ? niter : NM2;
-            for (int q = 0; q < nm0; q++) issue_mat(q, m_issued + q);
-            m_issued += nm0;
-        }
-        // planes 0..6 of the first x window (plane 7 is waited for in the first iteration)
-        bool fail = false;
-        for (int rp = 0; rp < 7 && !fail; rp++) {
-            const unsigned gi = rseq + rp;
-            if (mbar_wait(&rbar[gi % NR2], (gi / NR2) & 1u)) {
-                r_done = gi + 1;
-                if (top) image_plane(gi);
-            } else {
-                fail = true;
-            }
-        }
-        if (fail) {
-            abort2[sseq & 1] = 1;
-            atomicOr(&d_status, 1u);
-        }
-        __syncthreads();
-
-        float2 qx[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) qx[i] = bc2(0.0f);
-
-        for (int q = 0; q < niter; q++) {
-            const unsigned sq = sseq + q;
-            const long j = jstart + q;
-            const long P = j + 3;
-            // materials of the next lead plane into the stage the previous iteration finished with
-            if (tid == PRODUCER && q >= 1 && q + 1 < niter) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue_mat(q + 1, m_issued);
-                m_issued++;
-            }
-            bool ok_w = true;
-            {
-                const unsigned gi = rseq + q + 7;
-                ok_w = mbar_wait(&rbar[gi % NR2], (gi / NR2) & 1u);
-                if (ok_w) {
-                    r_done = gi + 1;
-                    if (top) image_plane(gi);  // lead plane four iterations on
-                }
-            }
-            {
-                const unsigned gm = mseq + q;
-                if (ok_w && mbar_wait(&mbar[gm % NM2], (gm / NM2) & 1u)) m_done = gm + 1;
-                else ok_w = false;
-            }
-            if (!ok_w) {
-                abort2[sq & 1] = 1;
-                atomicOr(&d_status, 1u);
-            }
-            // pass-2 inputs of plane j, read now and used after the barrier
-            const bool pass2 = j >= xbeg && own;
-            const long k = j * g.sx + (long)y * g.nz + z;
-            float2 c_old = bc2(0.0f), c_cur = bc2(0.0f), c_v = bc2(1.0f), c_q = bc2(0.0f), c_b = bc2(1.0f);
-            if (pass2) {
-                c_old = ld2((fld == 0 ? F.pold : F.mold) + k);  // written below: not the read-only path
-                c_cur = ldg2((fld == 0 ? F.pcur : F.mcur) + k);
-                c_v = ldg2(F.v + k);
-                c_q = ldg2(F.q + k);
-                c_b = ldg2(F.b + k);
-            }
-            // pass 1 at the lead plane
-            const float *ring[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) ring[i] = sm + O_RING + ((rseq + q + i) % NR2) * R_SLOT;
-            const float *mat = sm + O_MAT + ((mseq + q) % NM2) * MSTAGE;
-            float *yw = sm + O_YZ + ((sq + 3) % NS2) * YZ;  // y/z outputs of plane P
-            float *zw = yw + 2 * TYR * TZ;
-            const bool pin = P >= 4 && P < g.nx - 4;
-            float2 xo = bc2(0.0f);
-            if (tile_role) {
-                const Out6 c = pass1<TTI, 0>(g, ring, mat, row + 4, 4 + 2 * zp, pin && yz_tile, top && zp == 0);
-                xo = c.px;
-                st2(yw + (row + 4) * TZ + 2 * zp, c.py);
-                st2(yw + TYR * TZ + (row + 4) * TZ + 2 * zp, c.my);
-                st2(zw + row * TZW + 4 + 2 * zp, c.pz);
-                st2(zw + TY * TZW + row * TZW + 4 + 2 * zp, c.mz);
-                if (top && zp < 2) {
-                    // symmetric image t[-k] = t[k-1] of the z outputs above the free surface
-                    st2(zw + row * TZW + 2 - 2 * zp, make_float2(c.pz.y, c.pz.x));
-                    st2(zw + TY * TZW + row * TZW + 2 - 2 * zp, make_float2(c.mz.y, c.mz.x));
-                }
-                st2(MX + (sq & 1) * 512 + 2 * u, c.mx);
-            } else if (h_kind == 1) {
-                const Out6 h = pass1<TTI, 1>(g, ring, mat, h_er, h_ec, pin && yz_halo, top && h_zp == 0);
-                st2(yw + h_er * TZ + h_ec - 4, h.py);
-                st2(yw + TYR * TZ + h_er * TZ + h_ec - 4, h.my);
-            } else if (h_kind == 2 && !(top && h_ec < 4)) {
-                // (the z-halo pairs above the free surface hold images, written by the tile role)
-                const Out6 h = pass1<TTI, 2>(g, ring, mat, h_er, h_ec, pin && yz_halo, false);
-                st2(zw + (h_er - 4) * TZW + h_ec, h.pz);
-                st2(zw + TY * TZW + (h_er - 4) * TZW + h_ec, h.mz);
-            }
-            __syncthreads();
-            if (abort2[sq & 1]) {
-                stop = true;
-                break;
-            }
-            // the ring plane every thread has finished with (plane q) takes plane q + 9
-            if (tid == PRODUCER && q + NR2 < nplanes) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue_ring(q + NR2, r_issued);
-                r_issued++;
-            }
-            if (!tile_role) xo = ld2(MX + (sq & 1) * 512 + 2 * u);
-            float2 dx;
-            switch (q & 7) {
-                case 0: dx = xqueue<0>(g, qx, xo); break;
-                case 1: dx = xqueue<1>(g, qx, xo); break;
-                case 2: dx = xqueue<2>(g, qx, xo); break;
-                case 3: dx = xqueue<3>(g, qx, xo); break;
-                case 4: dx = xqueue<4>(g, qx, xo); break;
-                case 5: dx = xqueue<5>(g, qx, xo); break;
-                case 6: dx = xqueue<6>(g, qx, xo); break;
-                default: dx = xqueue<7>(g, qx, xo); break;
-            }
-            if (pass2) {
-                // pass 2 of this thread's field at plane j (prop3DAcoTTIDenQ_DEO2_FDTD.h:1420-1421)
-                const float *yr = sm + O_YZ + (sq % NS2) * YZ;  // outputs of plane j (lead plane three iterations ago)
-                const float *ty = yr + fld * TYR * TZ + row * TZ + 2 * zp;
-                const float2 dy = st8d(g, g.idy, ld2(ty), ld2(ty + TZ), ld2(ty + 2 * TZ), ld2(ty + 3 * TZ),
-                                       ld2(ty + 4 * TZ), ld2(ty + 5 * TZ), ld2(ty + 6 * TZ), ld2(ty + 7 * TZ));
-                float v[10];
-                load10(v, yr + 2 * TYR * TZ + fld * TY * TZW + row * TZW + 2 * zp);
-                const float2 dz = st8zd(g, g.idz, v, 0);
-                float2 L = add2(add2(dx, dy), dz);
-                if (top && zp == 0) L.x = 0.0f + 0.0f + 0.0f;  // free-surface row: every derivative is zero
-                const bool ok = j >= 4 && j < g.nx - 4 && yz_tile;
-                const float2 k2 = div2(mul2(mul2(bc2(g.dt2), c_v), c_v), c_b);
-                const float2 t = sub2(sub2(mul2(k2, L), mul2(c_q, sub2(c_cur, c_old))), c_old);
-                const float2 np = add2(t, mul2(bc2(2.0f), c_cur));
-                float2 nv = ok ? np : c_old;
-                if (F.epi.born_dv) {
-                    // Born-V injection fused after the step (prop3DAcoTTIDenQ_DEO2_FDTD.h:423-452):
-                    // new += 2 dt^2 dV/V * DP (DM), every cell
-                    const float2 fac = div2(mul2(bc2(2.0f * g.dt * g.dt), ldg2(F.epi.born_dv + k)), c_v);
-                    nv = add2(nv, mul2(fac, ldg2((fld == 0 ? F.epi.born_dp : F.epi.born_dm) + k)));
-                }
-                st2((fld == 0 ? F.pold : F.mold) + k, nv);
-                float2 sp = ok ? L : bc2(0.0f);
-                // ScaleSpatialDerivatives fused (.h:387-415): pSpace, mSpace *= V^2/B
-                if (F.epi.scale_space) sp = mul2(sp, div2(mul2(c_v, c_v), c_b));
-                st2((fld == 0 ? F.pspace : F.mspace) + k, sp);
-                if (fld == 0 && F.epi.img) {
-                    // imaging condition fused after the step (.h:567-592): img += 2B/V^3 (DP pOld +
-                    // DM mOld), pOld/mOld being this step's input pCur/mCur
-                    const float2 dp = ldg2(F.epi.img_dp + k), dm = ldg2(F.epi.img_dm + k), mc = ldg2(F.mcur + k);
-                    const float2 fac = div2(mul2(bc2(2.0f), c_b), mul2(mul2(c_v, c_v), c_v));
-                    float2 a = ld2(F.epi.img + k);
-                    a = add2(a, mul2(fac, add2(mul2(dp, c_cur), mul2(dm, mc))));
-                    st2(F.epi.img + k, a);
-                }
-                if (fld == 0 && F.illum) {
-                    // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add,
-                    // as illumination.c:31-53 does)
-                    float2 a = ld2(F.illum + k);
-                    a.x = __fadd_rn(a.x, __fmul_rn(c_cur.x, c_cur.x));
-                    a.y = __fadd_rn(a.y, __fmul_rn(c_cur.y, c_cur.y));
-                    st2(F.illum + k, a);
-                }
-            }
-        }
-        rseq += nplanes;
-        mseq += niter;
-        sseq += niter;
-    }
-    if (stop && tid == PRODUCER) {
-        // let copies still in flight land before the CTA leaves (bounded)
-        for (unsigned gi = r_done; gi < r_issued; gi++) mbar_wait(&rbar[gi % NR2], (gi / NR2) & 1u, 100000000ull);
-        for (unsigned gi = m_done; gi < m_issued; gi++) mbar_wait(&mbar[gi % NM2], (gi / NM2) & 1u, 100000000ull);
-    }
-}
-
 bool aniso_maps(const Grid &g, int phys, const Fields &F, CUtensorMap *m) {
     const float *srcs[15] = {F.pcur, F.mcur, F.b, F.eps, F.eta, F.f, F.st, F.ct, F.sp, F.cp,
                              F.pold, F.mold, F.v, F.q, F.b};
@@ -934,7 +629,8 @@ template <int PHYS, bool LINEAR>
 int aniso_grid_cap() {
     static int cap = 0;
     if (!cap) {
-        for (auto kern : {k_aniso3d_tma<PHYS, LINEAR, false>, k_aniso3d_tma<PHYS, LINEAR, true>})
+        for (auto kern : {k_aniso3d_tma<PHYS, LINEAR, false>, k_aniso3d_tma<PHYS, LINEAR, true>,
+                          k_aniso3d_tma<PHYS, LINEAR, false, true>})
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
@@ -943,58 +639,6 @@ int aniso_grid_cap() {
         cap = sms * (per > 0 ? per : 1);
     }
     return cap;
-}
-
-// x-chunk count for a persistent launch of `cap` CTAs over `tiles` (z,y) tiles: the fewest waves
-// of items, each chunk paying for its warm-up planes
-int pick_chunks(const Grid &g, long tiles, int cap) {
-    int best_nch = 1;
-    double best_cost = 1e30;
-    for (int nch = 1; nch <= 64 && nch <= g.nx / 16 + 1; nch++) {
-        const long chunk = (g.nx + nch - 1) / nch;
-        const long items = tiles * nch;
-        const double waves = (double)((items + cap - 1) / cap);
-        const double cost = waves * (double)(chunk + WARMUP * 0.6);
-        if (cost < best_cost) {
-            best_cost = cost;
-            best_nch = nch;
-        }
-    }
-    return best_nch;
-}
-
-bool launch_split(const Grid &g, const Fields &F, cudaStream_t s) {
-    AnisoMaps M;
-    if (!aniso_maps(g, TTI, F, M.m)) return false;
-    static int cap = 0;
-    if (!cap) {
-        cudaFuncSetAttribute(k_tti3d_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)split::SMEM2);
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tti3d_split, split::NT2, split::SMEM2);
-        cap = sms * (per > 0 ? per : 1);
-    }
-    const int ntz = (int)((g.nz + TZ - 1) / TZ);
-    const int nty = (int)((g.ny + TY - 1) / TY);
-    const long tiles = (long)ntz * nty;
-    const int nch0 = pick_chunks(g, tiles, cap);
-    const int xchunk = (int)((g.nx + nch0 - 1) / nch0);
-    const int nch = (int)((g.nx + xchunk - 1) / xchunk);
-    const long work = tiles * nch;
-    const int grid = (int)(work < cap ? work : cap);
-    k_tti3d_split<<<grid, split::NT2, split::SMEM2, s>>>(g, F, M, ntz, nty, nch, xchunk);
-    return true;
-}
-
-// the single-object TTI step kernel: the split-role kernel unless WAVEFD_B200_TTI_KERNEL=ring
-bool use_split_tti() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("WAVEFD_B200_TTI_KERNEL");
-        v = (e && e[0] == 'r') ? 0 : 1;
-    }
-    return v == 1;
 }
 
 template <int PHYS, bool LINEAR>
@@ -1021,8 +665,12 @@ bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
     const int nch = (int)((g.nx + xchunk - 1) / xchunk);
     const long work = tiles * nch;
     const int grid = (int)(work < grid_cap ? work : grid_cap);
-    k_aniso3d_tma<PHYS, LINEAR, false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr,
-                                                                    nullptr, 0, nullptr);
+    if (F.epi.born_dv || F.epi.img || F.epi.scale_space)
+        k_aniso3d_tma<PHYS, LINEAR, false, true><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr,
+                                                                              nullptr, nullptr, 0, nullptr);
+    else
+        k_aniso3d_tma<PHYS, LINEAR, false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr,
+                                                                        nullptr, nullptr, 0, nullptr);
     return true;
 }
 
@@ -1033,11 +681,6 @@ bool fused_aniso3d_tma(const Grid &g, int phys, int linear, const Fields &F, cud
     if (phys == TTI) return linear ? false : launch<TTI, false>(g, F, s);
     if (phys == VTI) return linear ? launch<VTI, true>(g, F, s) : launch<VTI, false>(g, F, s);
     return false;
-}
-
-bool fused_tti3d_split(const Grid &g, const Fields &F, cudaStream_t s) {
-    if (g.ndim != 3 || g.nz % 4 != 0 || !use_split_tti()) return false;
-    return launch_split(g, F, s);
 }
 
 bool aniso3d_tma_describe(const Grid &g, int phys, const Fields &F, int xchunk, AnisoShotDesc *d, TileInfo *t) {

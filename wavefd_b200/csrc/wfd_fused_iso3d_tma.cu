@@ -220,7 +220,7 @@ __device__ __forceinline__ void ext_stage(const Grid &g, const bool xin, const b
 
 // D- in y and z, the time update and the stores of this thread's 4 cells (fmask bit m: the
 // reference updates cell m, given x)
-template <int MODE>
+template <int MODE, bool EPI>
 __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const bool xin, const bool top, const int z,
                                           const int y, const unsigned fmask, const int zq, const int row,
                                           const float2 *sx, const float2 *pc, const float *st, const float *TYs,
@@ -282,9 +282,9 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
             np = keep2(fm, m0, np, pov);  // cells the reference leaves alone
             nl = keep2(fm, m0, nl, bc2(0.0f));
         }
-        if (epi && epi->scale_space)  // ScaleSpatialDerivatives fused (.h:269-291): pSpace *= V^2/B
+        if (EPI && epi->scale_space)  // ScaleSpatialDerivatives fused (.h:269-291): pSpace *= V^2/B
             nl = mul2(nl, div2(mul2(V, V), half2(b4, h)));
-        if (epi && epi->born_dv) {
+        if (EPI && epi->born_dv) {
             // Born-V injection fused after the step (prop3DAcoIsoDenQ_DEO2_FDTD.h:305-334), every cell:
             // new += dt^2 V^2/B * DP * (2 B dV / V^3)
             const long kc = j * g.sx + (long)y * g.nz + z + m0;
@@ -292,7 +292,7 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
             const float2 fv = div2(mul2(mul2(bc2(2.0f), B), ld2(epi->born_dv + kc)), mul2(mul2(V, V), V));
             np = add2(np, mul2(mul2(k2, ld2(epi->born_dp + kc)), fv));
         }
-        if (epi && epi->img) {
+        if (EPI && epi->img) {
             // imaging condition fused after the step (.h:518-546): img += 2B/V^3 DP pOld, pOld being
             // this step's input pCur
             const long kc = j * g.sx + (long)y * g.nz + z + m0;
@@ -348,7 +348,7 @@ __device__ __forceinline__ void queue_phase(float2 (&qp)[8][2], float2 (&qt)[8][
 // BATCH = true: many objects (shots) of different sizes; every item names its shot, whose sizes,
 // output pointers and tensor maps sit in a descriptor in global memory; CTAs take items from a
 // shared counter (dynamic scheduling over shots of uneven size, in the order the caller packed).
-template <bool BATCH>
+template <bool BATCH, bool EPI = false>
 __global__ void __launch_bounds__(NT, 3)
     k_iso3d_tma(Grid g0, Fields F, const __grid_constant__ IsoMaps M, int ntz0, int nty0, int nch0, int xchunk0,
                 const IsoShotDesc *__restrict__ shots, const int *__restrict__ sel, const int2 *__restrict__ items,
@@ -500,8 +500,8 @@ __global__ void __launch_bounds__(NT, 3)
                 // one code path for every tile (the selects are cheap, code size is not)
                 ext_stage<EDGE>(g, xin, tile_top, z0, emask, st, TYs, TZs);
                 __syncthreads();
-                if (own) fin_stage<EDGE>(g, j, xin, tile_top, z, y, fmask, zq, row, sx, pc, st, TYs, TZs, out_pold,
-                                          out_pspace, BATCH ? nullptr : F.illum, BATCH ? nullptr : &F.epi);
+                if (own) fin_stage<EDGE, EPI>(g, j, xin, tile_top, z, y, fmask, zq, row, sx, pc, st, TYs, TZs, out_pold,
+                                               out_pspace, BATCH ? nullptr : F.illum, EPI ? &F.epi : nullptr);
             }
             __syncthreads();
             if (*abort_flag) {
@@ -526,7 +526,7 @@ int iso_grid_cap() {
     static int cap = 0;
     if (!cap) {
         int dev = 0, sms = 0, per = 0;
-        for (auto kern : {k_iso3d_tma<false>, k_iso3d_tma<true>})
+        for (auto kern : {k_iso3d_tma<false>, k_iso3d_tma<true>, k_iso3d_tma<false, true>})
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -573,7 +573,11 @@ bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
     const int nch = (int)((g.nx + xchunk - 1) / xchunk);
     const long work = tiles * nch;
     const int grid = (int)(work < grid_cap ? work : grid_cap);
-    k_iso3d_tma<false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr, 0,
+if (F.epi.born_dv || F.epi.img || F.epi.scale_space)
+            k_iso3d_tma<false, true><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr, 0,
+                                                    nullptr);
+    else
+            k_iso3d_tma<false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr, 0,
                                                     nullptr);
     return true;
 }

@@ -277,7 +277,7 @@ __device__ __forceinline__ void queue_phase(const Grid &g, float2 (&qp)[8][2], f
     }
 }
 
-template <bool LINEAR, bool BATCH>
+template <bool LINEAR, bool BATCH, bool EPI = false>
 __global__ void __launch_bounds__(NT, 2)
     k_vti3d_tma(Grid g0, Fields F, const __grid_constant__ AnisoMaps M, int ntz0, int nty0, int nch0, int xchunk0,
                 const AnisoShotDesc *__restrict__ shots, const int *__restrict__ sel, const int2 *__restrict__ items,
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(NT, 2)
                     // Born-V injection fused after the step (prop3DAcoVTIDenQ_DEO2_FDTD.h:420-452):
                     // new += 2 dt^2 dV/V * DP (DM), every cell
                     float2 bfac = bc2(0.0f);
-                    if (!BATCH && F.epi.born_dv)
+                    if (EPI && F.epi.born_dv)
                         bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), __ldg(reinterpret_cast<const float2 *>(F.epi.born_dv + k))), V);
 #pragma unroll
                     for (int f = 0; f < 2; f++) {
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(NT, 2)
                         const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc[f], po))), po);
                         const float2 np = add2(t, mul2(bc2(2.0f), pc[f]));
                         float2 nv = make_float2(ok0 ? np.x : po.x, ok1 ? np.y : po.y);
-                        if (!BATCH && F.epi.born_dv) {
+                        if (EPI && F.epi.born_dv) {
                             const float *d = f == 0 ? F.epi.born_dp : F.epi.born_dm;
                             nv = add2(nv, mul2(bfac, __ldg(reinterpret_cast<const float2 *>(d + k))));
                         }
@@ -478,11 +478,11 @@ __global__ void __launch_bounds__(NT, 2)
                         if (!LINEAR) {
                             float2 sp = make_float2(ok0 ? L[f].x : 0.0f, ok1 ? L[f].y : 0.0f);
                             // ScaleSpatialDerivatives fused (.h:384-407): pSpace, mSpace *= V^2/B
-                            if (!BATCH && F.epi.scale_space) sp = mul2(sp, div2(mul2(V, V), B));
+                            if (EPI && F.epi.scale_space) sp = mul2(sp, div2(mul2(V, V), B));
                             st2((f == 0 ? o_ps : o_ms) + k, sp);
                         }
                     }
-                    if (!BATCH && F.epi.img) {
+                    if (EPI && F.epi.img) {
                         // imaging condition fused after the step (.h:564-589): img += 2B/V^3 (DP pOld +
                         // DM mOld), pOld/mOld being this step's input pCur/mCur
                         const float2 dp = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dp + k));
@@ -531,7 +531,7 @@ template <bool LINEAR>
 int vti_grid_cap() {
     static int cap = 0;
     if (!cap) {
-        for (auto kern : {k_vti3d_tma<LINEAR, false>, k_vti3d_tma<LINEAR, true>})
+        for (auto kern : {k_vti3d_tma<LINEAR, false>, k_vti3d_tma<LINEAR, true>, k_vti3d_tma<LINEAR, false, true>})
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
@@ -566,7 +566,11 @@ bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
     const int nch = (int)((g.nx + xchunk - 1) / xchunk);
     const long work = tiles * nch;
     const int grid = (int)(work < grid_cap ? work : grid_cap);
-    k_vti3d_tma<LINEAR, false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr,
+if (F.epi.born_dv || F.epi.img || F.epi.scale_space)
+            k_vti3d_tma<LINEAR, false, true><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr,
+                                                           0, nullptr);
+    else
+            k_vti3d_tma<LINEAR, false><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr,
                                                            0, nullptr);
     return true;
 }

@@ -117,7 +117,6 @@ struct TileInfo {
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \
-    bool fused_tti3d_split(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                   \
     bool vti3d_tma_describe(const wfd::Grid &g, const wfd::Fields &F, int xchunk, wfd::AnisoShotDesc *d, \
                             wfd::TileInfo *t);                                                           \
     void vti3d_tma_batch(const wfd::Grid &gc, const wfd::AnisoShotDesc *shots, const int *sel,          \

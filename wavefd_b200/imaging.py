@@ -61,8 +61,10 @@ class DeviceStore:
         self.buf = torch.empty((nsnap, nfields) + tuple(shape), device="cuda")
 
     def put(self, k, fields, stream):
-        for i, f in enumerate(fields):
-            self.buf[k, i].copy_(f, non_blocking=True)
+        import torch
+        with torch.cuda.stream(stream):  # behind the step that wrote the fields
+            for i, f in enumerate(fields):
+                self.buf[k, i].copy_(f, non_blocking=True)
 
     def get(self, k, stream):
         return [self.buf[k, i] for i in range(self.buf.shape[1])]
