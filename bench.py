@@ -511,13 +511,6 @@ def run_born(args, W):
         disk = {"s_per_shot": round(t_disk * W["nt"] / disk_steps, 3), "sample_steps": disk_steps,
                 "bytes_written": disk_bytes, "speedup_learned_vs_disk": round(t_disk / disk_steps / (t_codec / ns), 3),
                 "where": f"{tmpdir} (O_DIRECT where the file system allows)"}
-        # the same through cuFile (GPUDirect Storage where the platform has it)
-        gstore = imaging.DiskStore(W["shape"], disk_steps // every, 2,
-                                   os.path.join(tmpdir, f"wfd_born_gds_{os.getpid()}.snap"), direct=True, gds=True)
-        _, t_gds = imaging.born_image(shot, data, gstore, every=every, nt=disk_steps)
-        disk["cufile"] = {"transport": gstore.transport, "s_per_shot": round(t_gds * W["nt"] / disk_steps, 3),
-                          "speedup_learned_vs_disk": round(t_gds / disk_steps / (t_codec / ns), 3)}
-        gstore.close()
     else:
         disk = {"unavailable": f"less than {1.5 * disk_bytes / 1e9:.0f} GB free in {tmpdir}"}
     # image error at this shape: learned against exact FP32 snapshots kept in device memory, over as

@@ -382,9 +382,6 @@ int WFD_IllumAccumulate(float *accum, const float *field, long n, void *stream);
 #define WFD_SNAP_HOST 2   /* payloads are host memory: pwrite/pread only, no CUDA call */
 #define WFD_SNAP_DIRECT 4 /* O_DIRECT for payloads where the file system allows it */
 #define WFD_SNAP_CODEC 8  /* recorded in the header: the payloads are codec codes */
-#define WFD_SNAP_GDS 16   /* device payloads move between the device and the file through cuFile
-                             (GPUDirect Storage where the platform has it; implies O_DIRECT);
-                             without libcufile, or if cuFile refuses the file, staged transfers */
 void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, int flags);
 int WFD_Snap_Write(void *f, long ifield, const void *src, long nbytes, void *stream);
 /* start reading field ifield into a staging slot (a later Read of it only waits) */
@@ -393,9 +390,6 @@ int WFD_Snap_Read(void *f, long ifield, void *dst, long nbytes, void *stream);
 long WFD_Snap_Length(void *f, long ifield);
 long WFD_Snap_NumFields(void *f);
 int WFD_Snap_Flags(void *f);
-/* how device payloads move: 0 staged through pinned host memory, 1 cuFile's compatibility path
- * (no nvidia-fs driver), 2 GPUDirect Storage, 3 host payloads (WFD_SNAP_HOST); -1 null file */
-int WFD_Snap_Transport(void *f);
 /* wait for every transfer, then write the header (index) */
 int WFD_Snap_Sync(void *f);
 int WFD_Snap_Close(void *f);

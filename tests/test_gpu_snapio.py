@@ -17,21 +17,16 @@ def torch():
     return torch
 
 
-@pytest.mark.parametrize("direct", [False, True, "gds"])
+@pytest.mark.parametrize("direct", [False, True])
 def test_device_round_trip(torch, tmp_path, direct):
-    """direct="gds": transfers through cuFile (GPUDirect Storage where the platform has it, cuFile's
-    compatibility path otherwise; without libcufile the staged path), the same results bit for bit."""
     from wavefd_b200.snapio import SnapshotFile, read_index
-    gds = direct == "gds"
-    direct = bool(direct)
     p = tmp_path / "d.snap"
     g = torch.Generator(device="cuda").manual_seed(3)
     sizes = [1 << 20, (1 << 20) + 37, 123457, 1 << 18, 999, 1 << 20]
     ref = [torch.randn(n, device="cuda", generator=g) for n in sizes]
     s = torch.cuda.Stream()
     src = torch.empty(max(sizes), device="cuda")
-    with SnapshotFile(p, "w", len(sizes), 4 * max(sizes), direct=direct, gds=gds) as f:
-        print(f"snapshot transport: {f.transport}")
+    with SnapshotFile(p, "w", len(sizes), 4 * max(sizes), direct=direct) as f:
         with torch.cuda.stream(s):
             for i, r in enumerate(ref):
                 src[:r.numel()].copy_(r)
@@ -50,7 +45,7 @@ def test_device_round_trip(torch, tmp_path, direct):
     flags, nf, slot, data, idx = read_index(p)
     assert nf == len(sizes) and [ln for _, ln in idx] == [4 * n for n in sizes]
     # reopen for reading, random order
-    with SnapshotFile(p, "r", direct=direct, gds=gds) as f:
+    with SnapshotFile(p, "r", direct=direct) as f:
         for i in [2, 5, 0, 4, 1, 3]:
             o = torch.zeros_like(ref[i])
             f.read(i, o)

@@ -70,7 +70,6 @@ def _declare(lib):
     fn("WFD_Snap_Length", c_long, [c_void_p, c_long])
     fn("WFD_Snap_NumFields", c_long, [c_void_p])
     fn("WFD_Snap_Flags", c_int, [c_void_p])
-    fn("WFD_Snap_Transport", c_int, [c_void_p])
     fn("WFD_Snap_Sync", c_int, [c_void_p])
     fn("WFD_Snap_Close", c_int, [c_void_p])
     fn("WFD_Interp", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_long, c_long, c_long, c_long, c_void_p])

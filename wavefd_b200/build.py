@@ -80,7 +80,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         objs = list(ex.map(_compile, jobs))
     tmp = out + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "shared", "-o", tmp] + objs + ["-ldl"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "shared", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

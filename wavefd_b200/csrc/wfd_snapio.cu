@@ -18,15 +18,7 @@
 // and copy to a device staging slot on the copy stream, and the read itself is a device-to-device
 // copy on the caller's stream behind an event. Host payloads (WFD_SNAP_HOST) go straight through
 // pwrite()/pread() and make no CUDA call.
-//
-// GPU-direct transfers (WFD_SNAP_GDS): the worker moves payloads between the device staging slot and
-// the file with cuFile (libcufile, loaded at run time), no pinned host copy on the library's side:
-// GPUDirect Storage DMA where the nvidia-fs driver and the file system support it, cuFile's own
-// compatibility path otherwise (WFD_Snap_Transport says which). Without libcufile, or when cuFile
-// refuses the file, the file falls back to the staged transfers above.
 #include <cuda_runtime.h>
-#include <cufile.h>
-#include <dlfcn.h>
 #include <fcntl.h>
 #include <unistd.h>
 
@@ -56,46 +48,6 @@ constexpr int kStages = 3;
 constexpr auto kWaitLimit = std::chrono::seconds(600);  // a host wait for the worker gives up after this
 
 long round_up(long v, long a) { return (v + a - 1) / a * a; }
-
-// cuFile entry points, resolved once from libcufile (absent: ok = false, files use staged transfers)
-struct CuFile {
-    bool ok = false;
-    unsigned nvfs_major = 0;  // 0: no nvidia-fs driver (cuFile's compatibility path)
-    CUfileError_t (*handle_register)(CUfileHandle_t *, CUfileDescr_t *) = nullptr;
-    void (*handle_deregister)(CUfileHandle_t) = nullptr;
-    ssize_t (*read)(CUfileHandle_t, void *, size_t, off_t, off_t) = nullptr;
-    ssize_t (*write)(CUfileHandle_t, const void *, size_t, off_t, off_t) = nullptr;
-    CUfileError_t (*buf_register)(const void *, size_t, int) = nullptr;
-    CUfileError_t (*buf_deregister)(const void *) = nullptr;
-};
-
-const CuFile &cufile() {
-    static const CuFile api = [] {
-        CuFile a;
-        void *h = dlopen("libcufile.so.0", RTLD_NOW | RTLD_LOCAL);
-        if (!h) h = dlopen("libcufile.so", RTLD_NOW | RTLD_LOCAL);
-        if (!h) return a;
-        auto sym = [&](const char *n) { return dlsym(h, n); };
-        auto open_fn = reinterpret_cast<CUfileError_t (*)(void)>(sym("cuFileDriverOpen"));
-        auto props_fn = reinterpret_cast<CUfileError_t (*)(CUfileDrvProps_t *)>(sym("cuFileDriverGetProperties"));
-        a.handle_register = reinterpret_cast<decltype(a.handle_register)>(sym("cuFileHandleRegister"));
-        a.handle_deregister = reinterpret_cast<decltype(a.handle_deregister)>(sym("cuFileHandleDeregister"));
-        a.read = reinterpret_cast<decltype(a.read)>(sym("cuFileRead"));
-        a.write = reinterpret_cast<decltype(a.write)>(sym("cuFileWrite"));
-        a.buf_register = reinterpret_cast<decltype(a.buf_register)>(sym("cuFileBufRegister"));
-        a.buf_deregister = reinterpret_cast<decltype(a.buf_deregister)>(sym("cuFileBufDeregister"));
-        if (!open_fn || !a.handle_register || !a.handle_deregister || !a.read || !a.write) return a;
-        if (open_fn().err != CU_FILE_SUCCESS) return a;  // the driver stays open for the process
-        if (props_fn) {
-            CUfileDrvProps_t pr;
-            std::memset(&pr, 0, sizeof pr);
-            if (props_fn(&pr).err == CU_FILE_SUCCESS) a.nvfs_major = pr.nvfs.major_version;
-        }
-        a.ok = true;
-        return a;
-    }();
-    return api;
-}
 long header_bytes(long nfields) { return round_up(48 + 16 * nfields, kAlign); }
 
 enum class St { FREE, WRITE, READ, READY };
@@ -120,8 +72,6 @@ struct File {
     std::string path;
     int fd = -1;
     bool host_mode = false, readonly = false, direct = false;
-    bool gds = false;               // payloads through cuFile (WFD_SNAP_GDS accepted)
-    CUfileHandle_t cf = nullptr;
     uint32_t flags = 0;
     long nfields = 0, slot = 0, hdr = 0;
     std::vector<long> len;
@@ -222,63 +172,6 @@ void worker_main(File *f) {
             f->jobs.pop_front();
         }
         Stage &s = f->stage[job.stage];
-        if (f->gds) {
-            // device slot <-> file through cuFile, whole 4096-byte blocks (the slot is that large)
-            const CuFile &cf = cufile();
-            const long n = round_up(s.nbytes, kAlign);
-            const long off = f->hdr + s.field * f->slot;
-            bool ok = true;
-            cudaError_t e = cudaSuccess;
-            if (job.write) {
-                e = cudaEventSynchronize(s.staged_ev);  // the caller's copy into the slot
-                if (e != cudaSuccess) {
-                    cuda_fail(f, e, "WFD_Snap_Write (copy to the slot)");
-                    ok = false;
-                }
-                if (ok) {
-                    errno = 0;
-                    const ssize_t done = cf.write(f->cf, s.dev, (size_t)n, (off_t)off, 0);
-                    if (done != n) {
-                        fail(f, WFD_ERR_IO, io_message(f, "wrote (cuFile)", done < 0 ? 0 : done, n, s.field));
-                        ok = false;
-                    }
-                }
-            } else {
-                if (s.dev_free_set) e = cudaEventSynchronize(s.dev_free_ev);  // the slot's last reader
-                if (e != cudaSuccess) {
-                    cuda_fail(f, e, "WFD_Snap_Read (previous copy)");
-                    ok = false;
-                }
-                if (ok) {
-                    errno = 0;
-                    const ssize_t done = cf.read(f->cf, s.dev, (size_t)n, (off_t)off, 0);
-                    if (done < s.nbytes) {
-                        fail(f, WFD_ERR_IO, io_message(f, "read (cuFile)", done < 0 ? 0 : done, s.nbytes, s.field));
-                        ok = false;
-                    }
-                }
-            }
-            // the slot is free (write) or holds the field (read) now: mark it with an event on the idle
-            // copy stream, which the next copy into or out of the slot waits for
-            if (ok) ok = (e = cudaEventRecord(job.write ? s.dev_free_ev : s.host_ev, f->copy)) == cudaSuccess;
-            if (!ok && e != cudaSuccess) cuda_fail(f, e, "WFD_Snap (event)");
-            std::lock_guard<std::mutex> lk(f->mu);
-            if (job.write) {
-                if (ok) f->len[s.field] = s.nbytes;
-                s.dev_free_set = ok;
-                s.st = St::FREE;
-                s.field = -1;
-            } else {
-                s.host_ev_set = ok;
-                if (ok) s.st = St::READY;
-                else {
-                    s.st = St::FREE;
-                    s.field = -1;
-                }
-            }
-            f->cv_done.notify_all();
-            continue;
-        }
         if (job.write) {
             // the pinned copy has landed once the D2H copy is done
             cudaError_t e = cudaEventSynchronize(s.host_ev);
@@ -391,13 +284,6 @@ void destroy(File *f) {
         f->cv_job.notify_all();
         f->worker.join();
     }
-    if (f->cf) {
-        const CuFile &cf = cufile();
-        for (auto &s : f->stage)
-            if (s.dev && cf.buf_deregister) cf.buf_deregister(s.dev);
-        cf.handle_deregister(f->cf);
-        f->cf = nullptr;
-    }
     if (!f->host_mode) {
         for (auto &s : f->stage) {
             if (s.host) cudaFreeHost(s.host);
@@ -427,8 +313,7 @@ extern "C" void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, i
     f->path = path;
     f->host_mode = (flags & WFD_SNAP_HOST) != 0;
     f->readonly = (flags & WFD_SNAP_READ) != 0;
-    f->gds = (flags & WFD_SNAP_GDS) != 0 && !f->host_mode && cufile().ok;
-    f->direct = ((flags & WFD_SNAP_DIRECT) != 0 || f->gds) && !f->host_mode;
+    f->direct = (flags & WFD_SNAP_DIRECT) != 0 && !f->host_mode;
     if (f->readonly) {
         f->fd = open(path, O_RDONLY);  // the header is read through the page cache
         if (f->fd < 0) {
@@ -497,22 +382,11 @@ extern "C" void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, i
         f->flags = (uint32_t)(flags & WFD_SNAP_CODEC);
         f->len.assign((size_t)nfields, -1);
     }
-    if (f->gds) {
-        // cuFile takes the O_DIRECT descriptor; a file it refuses uses the staged transfers
-        CUfileDescr_t d;
-        std::memset(&d, 0, sizeof d);
-        d.type = CU_FILE_HANDLE_TYPE_OPAQUE_FD;
-        d.handle.fd = f->fd;
-        if (!f->direct || cufile().handle_register(&f->cf, &d).err != CU_FILE_SUCCESS) {
-            f->cf = nullptr;
-            f->gds = false;
-        }
-    }
     if (!f->host_mode) {
         cudaError_t e = cudaGetDevice(&f->device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->copy, cudaStreamNonBlocking);
         for (auto &s : f->stage) {
-            if (e == cudaSuccess && !f->gds) e = cudaHostAlloc(&s.host, (size_t)f->slot, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaHostAlloc(&s.host, (size_t)f->slot, cudaHostAllocDefault);
             if (e == cudaSuccess) e = wfd::dMalloc(&s.dev, (size_t)f->slot);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.host_ev, cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.dev_free_ev, cudaEventDisableTiming);
@@ -524,20 +398,9 @@ extern "C" void *WFD_Snap_Open(const char *path, long nfields, long max_bytes, i
             destroy(f);
             return nullptr;
         }
-        if (f->gds && cufile().buf_register)
-            for (auto &st : f->stage) cufile().buf_register(st.dev, (size_t)f->slot, 0);  // optional
         f->worker = std::thread(worker_main, f);
     }
     return f;
-}
-
-extern "C" int WFD_Snap_Transport(void *fp) {
-    using namespace wfd::snap;
-    const File *f = static_cast<const File *>(fp);
-    if (!f) return -1;
-    if (f->host_mode) return 3;
-    if (!f->gds) return 0;
-    return cufile().nvfs_major > 0 ? 2 : 1;
 }
 
 extern "C" int WFD_Snap_Write(void *fp, long ifield, const void *src, long nbytes, void *stream) {
@@ -577,19 +440,6 @@ extern "C" int WFD_Snap_Write(void *fp, long ifield, const void *src, long nbyte
     if (e == cudaSuccess && s.host_ev_set) e = cudaStreamWaitEvent(st, s.host_ev, 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.dev, src, (size_t)nbytes, cudaMemcpyDefault, st);
     if (e == cudaSuccess) e = cudaEventRecord(s.staged_ev, st);
-    if (f->gds) {  // the worker writes the slot to the file once the copy into it is done
-        if (e != cudaSuccess) {
-            lk.unlock();
-            return cuda_fail(f, e, "WFD_Snap_Write");
-        }
-        s.dev_free_set = false;  // set again by the worker when the slot's write is done
-        s.st = St::WRITE;
-        s.field = ifield;
-        s.nbytes = nbytes;
-        f->jobs.push_back({true, si});
-        f->cv_job.notify_one();
-        return WFD_OK;
-    }
     if (e == cudaSuccess) e = cudaStreamWaitEvent(f->copy, s.staged_ev, 0);
     if (e == cudaSuccess && s.host_ev_set) e = cudaStreamWaitEvent(f->copy, s.host_ev, 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.host, s.dev, (size_t)nbytes, cudaMemcpyDeviceToHost, f->copy);

@@ -168,13 +168,12 @@ class DiskStore:
     the disk write runs behind it); a get reads snapshot k into the store's device arrays on the
     adjoint stream and starts reading snapshot k - 1 (the adjoint asks in decreasing order)."""
 
-    def __init__(self, shape, nsnap, nfields, path, direct=False, keep=False, gds=False):
+    def __init__(self, shape, nsnap, nfields, path, direct=False, keep=False):
         import torch
         from .snapio import SnapshotFile
         self.shape, self.nf, self.path, self.keep = tuple(shape), nfields, str(path), keep
         self.field_bytes = int(np.prod(self.shape)) * 4
-        self.file = SnapshotFile(self.path, "w", nsnap * nfields, self.field_bytes, direct=direct, gds=gds)
-        self.transport = self.file.transport
+        self.file = SnapshotFile(self.path, "w", nsnap * nfields, self.field_bytes, direct=direct)
         self.out = [torch.empty(self.shape, device="cuda") for _ in range(nfields)]
         self.nsnap = nsnap
 

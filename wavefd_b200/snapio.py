@@ -4,9 +4,7 @@ The role of `Compressor` / `compressedwrite` / `compressedread!` (src/compressed
 forward run writes field i of the file once, the adjoint run reads the fields back in any order.
 The work is done by the library's `WFD_Snap_*` entry points (wavefd_b200/csrc/wfd_snapio.cu):
 device arrays move through device and pinned staging and a worker thread's pwrite/pread, ordered
-on the caller's CUDA stream (or, with gds=True, between the device staging slot and the file through
-cuFile: GPUDirect Storage where the platform supports it); host arrays (numpy) go straight through
-pwrite/pread.
+on the caller's CUDA stream; host arrays (numpy) go straight through pwrite/pread.
 
 File layout (little-endian): a header of a multiple of 4096 bytes ("WFDSNAP1", u32 version, u32
 flags, i64 nfields, i64 slot, i64 data offset, then per field i64 offset and i64 length, -1 =
@@ -20,9 +18,7 @@ import numpy as np
 
 from . import _lib
 
-READ, HOST, DIRECT, CODEC, GDS = 1, 2, 4, 8, 16
-TRANSPORTS = {0: "staged through pinned host memory", 1: "cuFile (compatibility path, no nvidia-fs)",
-              2: "GPUDirect Storage (cuFile, nvidia-fs)", 3: "host arrays"}
+READ, HOST, DIRECT, CODEC = 1, 2, 4, 8
 MAGIC = b"WFDSNAP1"
 
 
@@ -41,13 +37,11 @@ class SnapshotFile:
     """Open a snapshot file. mode "w": create (or truncate) with `nfields` slots of up to
     `max_bytes` each; mode "r": open an existing file. host=True: the arrays are numpy arrays
     (no CUDA use); otherwise CUDA tensors, with the transfers ordered on `stream` (a
-    torch.cuda.Stream, default the current one). direct=True asks for O_DIRECT; gds=True for
-    transfers through cuFile (see `transport`)."""
+    torch.cuda.Stream, default the current one). direct=True asks for O_DIRECT."""
 
-    def __init__(self, path, mode="w", nfields=0, max_bytes=0, host=False, direct=False, codec=False, gds=False):
+    def __init__(self, path, mode="w", nfields=0, max_bytes=0, host=False, direct=False, codec=False):
         self.lib = _lib.library()
-        flags = ((READ if mode == "r" else 0) | (HOST if host else 0) | (DIRECT if direct else 0) |
-                 (CODEC if codec else 0) | (GDS if gds else 0))
+        flags = (READ if mode == "r" else 0) | (HOST if host else 0) | (DIRECT if direct else 0) | (CODEC if codec else 0)
         self.host = host
         self.path = str(path)
         self.f = self.lib.WFD_Snap_Open(self.path.encode(), int(nfields), int(max_bytes), flags)
@@ -68,11 +62,6 @@ class SnapshotFile:
     @property
     def flags(self):
         return self.lib.WFD_Snap_Flags(self.f)
-
-    @property
-    def transport(self):
-        """How device payloads move (TRANSPORTS)."""
-        return TRANSPORTS.get(self.lib.WFD_Snap_Transport(self.f), "unknown")
 
     def length(self, i):
         return self.lib.WFD_Snap_Length(self.f, int(i))
