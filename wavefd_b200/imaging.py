@@ -200,10 +200,10 @@ class DiskStore:
 
 
 def make_shot(physics, shape, seed=0, d=10.0, dt=0.0005, nsponge=40, fpeak=12.0, nt=1000, nrec=(32, 32),
-              perturbation=True):
+              perturbation=True, horizons=(0.15, 0.9)):
     """Seeded shot: the earth model (device tensors), a Hicks source at the centre near the surface, a
     surface receiver grid, the causal Ricker wavelet, and the Born velocity perturbation (+-2 % on 20
-    horizons, sparse) used as the reflectivity of the data."""
+    horizons between the given fractions of the depth, sparse) used as the reflectivity of the data."""
     import torch
     from .spacetime import causal_ricker
     model = synthetic.earth_model(shape, physics, seed=seed, d=d, dt=dt, nsponge=nsponge, device="cuda")
@@ -215,7 +215,7 @@ def make_shot(physics, shape, seed=0, d=10.0, dt=0.0005, nsponge=40, fpeak=12.0,
         nx, ny, nz = shape
         rng = np.random.default_rng(seed + 1000)
         dv = torch.zeros(shape, device="cuda")
-        for z in np.linspace(nz * 0.15, nz * 0.9, 20).astype(int):
+        for z in np.linspace(nz * horizons[0], nz * horizons[1], 20).astype(int):
             mask = torch.from_numpy((rng.random((nx, ny)) < 0.1).astype(np.float32)).cuda()
             dv[:, :, z] = mask * model["V"][:, :, z] * float(rng.choice([-0.02, 0.02]))
     return dict(model=model, src=src, rec=rec, wavelet=wav, dv=dv, shape=tuple(shape), d=d, dt=dt, nsponge=nsponge,
