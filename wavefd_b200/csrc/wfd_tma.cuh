@@ -49,12 +49,25 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 static __device__ uint64_t d_pipeline_wait_ns = 2000000000ull;
 
 // Bounded wait for the phase with the given parity to complete; false on timeout. Without an
-// explicit limit the pipeline limit applies (read only once the first poll has failed).
+// explicit limit the pipeline limit applies (read only once the first poll has failed). The first
+// poll does not block (test_wait); the later ones let the hardware suspend the thread (try_wait).
+// A limit of 1 ns (the test hook) gives up at the first poll that finds the copy still in flight:
+// a blocking poll would sleep until the copy lands, and the timer may not advance within 1 ns.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, uint64_t limit_ns = 0) {
     const uint32_t addr = smem_u32(bar);
     uint32_t ok = 0;
-    uint64_t t0 = 0;
-    for (int spin = 0;; spin++) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    const uint64_t t0 = globaltimer_ns();
+    if (limit_ns == 0) limit_ns = *(volatile uint64_t *)&d_pipeline_wait_ns;
+    if (limit_ns <= 1) return false;
+    for (;;) {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -63,12 +76,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, uint64
             : "r"(addr), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (spin == 0) {
-            t0 = globaltimer_ns();
-            if (limit_ns == 0) limit_ns = *(volatile uint64_t *)&d_pipeline_wait_ns;
-        } else if (globaltimer_ns() - t0 > limit_ns) {
-            return false;
-        }
+        if (globaltimer_ns() - t0 > limit_ns) return false;
     }
 }
 
