@@ -469,13 +469,19 @@ def run_codec(args, W):
     code = codec.empty_code(shape)
     out = torch.empty(shape, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # larger than L2
-    for _ in range(max(3, args.warmup)):
-        codec.encode(f, shape, code)
-        codec.decode(code, shape, out)
-    torch.cuda.synchronize()
-    te, td = [], []
+    cb = codec.code_bytes(shape)
+    peak, peak_src = peaks()
+    bytes_e = 4 * n + cb  # read the field, write the code (the raw-block copy reads 1 % again)
+    bytes_d = 4 * n + cb
     K = args.steps
-    with ClockSampler(0) as clk:
+
+    def time_engine(name):
+        codec.engine = name
+        for _ in range(max(3, args.warmup)):
+            codec.encode(f, shape, code)
+            codec.decode(code, shape, out)
+        torch.cuda.synchronize()
+        te, td = [], []
         for _ in range(K):
             flush.zero_()
             e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
@@ -489,13 +495,19 @@ def run_codec(args, W):
             e3.synchronize()
             te.append(e0.elapsed_time(e1))
             td.append(e2.elapsed_time(e3))
-    cb = codec.code_bytes(shape)
-    ms_e, ms_d = statistics.median(te), statistics.median(td)
-    peak, peak_src = peaks()
-    bytes_e = 4 * n + cb  # read the field, write the code (the raw-block copy reads 1 % again)
-    bytes_d = 4 * n + cb
-    ach_e = bytes_e / (ms_e / 1e3) / 1e9
-    ach_d = bytes_d / (ms_d / 1e3) / 1e9
+        codec.status()
+        rel = float(torch.linalg.norm(out - f) / torch.linalg.norm(f))
+        ms_e, ms_d = statistics.median(te), statistics.median(td)
+        ach_e, ach_d = bytes_e / (ms_e / 1e3) / 1e9, bytes_d / (ms_d / 1e3) / 1e9
+        return {"encode": {"ms": round(ms_e, 4), "GB_s": round(ach_e, 1), "frac": round(ach_e / peak, 4)},
+                "decode": {"ms": round(ms_d, 4), "GB_s": round(ach_d, 1), "frac": round(ach_d / peak, 4)},
+                "field_rel_l2": rel}
+
+    with ClockSampler(0) as clk:
+        legacy = time_engine("mma.sync")
+        umma = time_engine("tcgen05")
+    ms_e, ms_d = umma["encode"]["ms"], umma["decode"]["ms"]
+    ach_e = umma["encode"]["GB_s"]
     out_j = {
         "metric": "learned codec throughput (encode + decode of one field)", "value": round(n / ((ms_e + ms_d) / 1e3) / 1e6, 1),
         "unit": "Mcells/s", "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_e + ms_d, 4),
@@ -503,11 +515,11 @@ def run_codec(args, W):
         "data": "synthetic smoothed random field", "config": {"workload": W["label"], "grid": list(shape),
                                                               "l2": "L2 flushed (256 MB write) before each launch"},
         "code_bytes": cb, "compression_ratio_bytes": round(4 * n / cb, 2),
-        "encode": {"ms": round(ms_e, 4), "GB_s": round(ach_e, 1), "frac": round(ach_e / peak, 4)},
-        "decode": {"ms": round(ms_d, 4), "GB_s": round(ach_d, 1), "frac": round(ach_d / peak, 4)},
+        "encode": umma["encode"], "decode": umma["decode"], "field_rel_l2": umma["field_rel_l2"],
+        "engines": {"tcgen05": umma, "mma.sync": legacy},
         "roofline": {"bound": "hbm", "achieved": round(ach_e, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(ach_e / peak, 4), "traffic": None, "kernel": "k_encode (+ raw-block selection)",
-                     "peak_source": peak_src},
+                     "frac": round(ach_e / peak, 4), "traffic": None,
+                     "kernel": "k_encode_umma (tcgen05; + raw-block selection)", "peak_source": peak_src},
         "e2e": {"value": round(n / ((ms_e + ms_d) / 1e3) / 1e6, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "clocks": clk.summary(),

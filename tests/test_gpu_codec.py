@@ -61,9 +61,11 @@ def test_gradient_matches_oracle(torch):
         assert r <= 10 * GRAD_TOL, (name, r)
 
 
-def test_encode_decode_matches_oracle(torch):
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+def test_encode_decode_matches_oracle(torch, engine):
     from wavefd_b200.codec import WavefieldCodec
     codec = WavefieldCodec(seed=7)
+    codec.engine = engine
     rng = np.random.default_rng(8)
     for shape in [(40, 36, 72), (21, 30, 45)]:  # partial slabs; nz not a multiple of 4 in the second
         f = rng.standard_normal(shape)
@@ -75,7 +77,7 @@ def test_encode_decode_matches_oracle(torch):
         out = torch.empty(shape, device="cuda")
         codec.encode(d_f, shape, code)
         codec.decode(code, shape, out)
-        torch.cuda.synchronize()
+        codec.status()  # no tensor-core completion wait ran out
         g = out.cpu().numpy().astype(np.float64)
         ref = co.roundtrip(codec.params, f)
         B, _ = co.blocks_of(f)
@@ -92,6 +94,43 @@ def test_encode_decode_matches_oracle(torch):
         # the raw blocks are the worst-coded ones (up to the histogram's 1/8-octave bins)
         err = ((Br.astype(np.float64) - B) ** 2).sum(1)
         assert err[raw].min() >= np.sort(err)[-cap] / 2.0
+
+
+def test_tcgen05_engine_matches_mma_sync(torch):
+    """The tcgen05 kernels (UMMA, accumulators in tensor memory) against the mma.sync ones on the same
+    weights and field: the same BF16 roundings, so the codes agree up to a rare last-bit difference
+    (a sum formed in another order rounds to the neighbouring BF16 value) and the decoded fields agree
+    to BF16 accuracy; a grid with partial slabs in every direction."""
+    from wavefd_b200.codec import WavefieldCodec
+    codec = WavefieldCodec(seed=9)
+    assert codec.engine == "tcgen05"
+    shape = (70, 45, 100)
+    rng = np.random.default_rng(10)
+    f = rng.standard_normal(shape)
+    for ax in range(3):
+        for _ in range(2):
+            f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
+    d_f = torch.from_numpy(f.astype(np.float32)).cuda()
+    outs, codes = {}, {}
+    for engine in ("tcgen05", "mma.sync"):
+        codec.engine = engine
+        code = codec.empty_code(shape)
+        out = torch.empty(shape, device="cuda")
+        codec.encode(d_f, shape, code)
+        codec.decode(code, shape, out)
+        codec.status()
+        outs[engine], codes[engine] = out.double(), code.clone()
+    a, b = outs["tcgen05"], outs["mma.sync"]
+    rel = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    assert rel <= 5e-3, rel
+    for o in outs.values():
+        assert bool(torch.isfinite(o).all())
+    # cross decoding: codes of one engine decoded by the other
+    codec.engine = "mma.sync"
+    cross = torch.empty(shape, device="cuda")
+    codec.decode(codes["tcgen05"], shape, cross)
+    codec.status()
+    assert float(torch.linalg.norm(cross.double() - a) / torch.linalg.norm(a)) <= 5e-3
 
 
 def test_training_reduces_loss(trained):

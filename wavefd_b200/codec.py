@@ -43,6 +43,9 @@ def _L():
         fn("WFD_Codec_Encode", c_int, [c_void_p, c_void_p, c_long, c_long, c_long, c_void_p, c_void_p])
         fn("WFD_Codec_Decode", c_int, [c_void_p, c_void_p, c_long, c_long, c_long, c_void_p, c_void_p])
         fn("WFD_Codec_RawBlocks", c_long, [c_void_p, c_long, c_long, c_long])
+        fn("WFD_Codec_SetEngine", c_int, [c_void_p, c_int])
+        fn("WFD_Codec_Engine", c_int, [c_void_p])
+        fn("WFD_Codec_Status", c_int, [c_void_p])
         fn("WFD_Codec_GatherBlocks", c_int, [c_void_p, c_long, c_long, c_long, c_void_p, c_long, c_void_p, c_void_p,
                                              c_void_p])
         fn("WFD_Codec_TrainStep", c_int, [c_void_p, c_void_p, c_long, c_float, POINTER(c_float), c_void_p])
@@ -111,6 +114,19 @@ class WavefieldCodec:
     def raw_blocks(self, code, shape) -> int:
         nx, ny, nz = shape
         return int(_L().WFD_Codec_RawBlocks(_dp(code), nx, ny, nz))
+
+    @property
+    def engine(self) -> str:
+        """"tcgen05" (UMMA with the accumulators in tensor memory, the default) or "mma.sync"."""
+        return "tcgen05" if _L().WFD_Codec_Engine(self.c) == 1 else "mma.sync"
+
+    @engine.setter
+    def engine(self, name: str):
+        _check(_L().WFD_Codec_SetEngine(self.c, {"tcgen05": 1, "mma.sync": 0}[name]), "SetEngine")
+
+    def status(self):
+        """Synchronises the device; raises if a tensor-core completion wait ran out."""
+        _check(_L().WFD_Codec_Status(self.c), "Status")
 
     # -- training -----------------------------------------------------------------------------------
     def train_step(self, blocks, lr: float) -> float:

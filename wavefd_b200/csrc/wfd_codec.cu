@@ -41,6 +41,8 @@
 #include "wavefd_b200.h"
 #include "wfd_alloc.h"
 #include "wfd_prop.h"
+#include "wfd_tma.cuh"
+#include "wfd_umma.cuh"
 
 namespace wfd {
 namespace codec {
@@ -569,6 +571,8 @@ constexpr size_t ENC_SMEM = (size_t)(2 * SLAB + 16 * 4 + 32 + 128 + 64) * 4 +
 constexpr size_t DEC_SMEM =
     (size_t)(SLAB + 16 + 128 + 64) * 4 + (size_t)(16 * LATP + 16 * HROW + 128 * W3P + 64 * W4P) * 2;
 
+#include "wfd_codec_umma.cuh"
+
 // ---- training blocks --------------------------------------------------------------------------------
 // blocks[i] = field block at origin (ox, oy, oz)[i] in the codec's cell order, divided by its max
 // |value| (zero blocks stay zero); scale[i] = that max. Cells outside the grid read as zero.
@@ -782,6 +786,8 @@ struct Codec {
     long step = 0;
     int device = 0;
     int grid_enc = 0, grid_dec = 0, grid_train = 0;
+    int engine = 1;  // encode/decode on 1: tcgen05 (UMMA, tensor memory), 0: mma.sync
+    int grid_enc_u = 0, grid_dec_u = 0;
 };
 
 Dims dims(long nx, long ny, long nz) {
@@ -896,6 +902,21 @@ extern "C" void *WFD_Codec_Create(unsigned seed) {
     c->grid_enc = sms * (pe > 0 ? pe : 1);
     c->grid_dec = sms * (pd > 0 ? pd : 1);
     c->grid_train = sms * (pt > 0 ? pt : 1);
+    // tcgen05 encode/decode: each CTA holds 64 tensor-memory columns, so up to 8 CTAs per SM fit the
+    // 512 columns; shared memory allows 2 encode and 4 decode CTAs
+    int peu = 0, pdu = 0;
+    const bool umma_ok =
+        cudaFuncSetAttribute(k_encode_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, umma_layout::E_BYTES) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_decode_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, umma_layout::D_BYTES) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&peu, k_encode_umma, NTC, umma_layout::E_BYTES) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pdu, k_decode_umma, NTC, umma_layout::D_BYTES) == cudaSuccess &&
+        peu > 0 && pdu > 0;
+    c->grid_enc_u = umma_ok ? sms * (peu < 8 ? peu : 8) : 0;
+    c->grid_dec_u = umma_ok ? sms * (pdu < 8 ? pdu : 8) : 0;
+    const char *eng = getenv("WAVEFD_B200_CODEC");
+    c->engine = umma_ok && !(eng && strcmp(eng, "mma") == 0) ? 1 : 0;
     if (cuda_status(cudaDeviceSynchronize(), "WFD_Codec_Create")) {
         WFD_Codec_Free(c);
         return nullptr;
@@ -949,7 +970,11 @@ extern "C" int WFD_Codec_Encode(void *codec, const float *field, long nx, long n
     const long nslab = (long)d.nsx * d.nsy * d.nsz;
     const int grid = (int)(nslab < c->grid_enc ? nslab : c->grid_enc);
     cudaMemsetAsync(base, 0, L.scale, st);  // ctl and histogram
-    k_encode<<<grid, NTC, ENC_SMEM, st>>>(d, field, c->wb, c->w, scale, err, lat);
+    if (c->engine == 1)
+        k_encode_umma<<<(int)(nslab < c->grid_enc_u ? nslab : c->grid_enc_u), NTC, umma_layout::E_BYTES, st>>>(
+            d, field, c->wb, c->w, scale, err, lat);
+    else
+        k_encode<<<grid, NTC, ENC_SMEM, st>>>(d, field, c->wb, c->w, scale, err, lat);
     const int gb = (int)((nb + 255) / 256 < 1184 ? (nb + 255) / 256 : 1184);
     k_err_hist<<<gb, 256, 0, st>>>(nb, err, hist);
     k_err_threshold<<<1, 1024, 0, st>>>(hist, cap, ctl);
@@ -975,9 +1000,36 @@ extern "C" int WFD_Codec_Decode(void *codec, const void *latent, long nx, long n
     const float *raw = reinterpret_cast<const float *>(base + L.raw);
     const long nslab = (long)d.nsx * d.nsy * d.nsz;
     const int grid = (int)(nslab < c->grid_dec ? nslab : c->grid_dec);
-    k_decode<<<grid, NTC, DEC_SMEM, st>>>(d, scale, lat, c->wb, c->w, field);
+    if (c->engine == 1)
+        k_decode_umma<<<(int)(nslab < c->grid_dec_u ? nslab : c->grid_dec_u), NTC, umma_layout::D_BYTES, st>>>(
+            d, scale, lat, c->wb, c->w, field);
+    else
+        k_decode<<<grid, NTC, DEC_SMEM, st>>>(d, scale, lat, c->wb, c->w, field);
     k_raw_scatter<<<(unsigned)(cap < 1184 ? cap : 1184), 128, 0, st>>>(d, ctl, cap, raw_id, raw, field);
     return cuda_status(cudaGetLastError(), "WFD_Codec_Decode");
+}
+
+extern "C" int WFD_Codec_SetEngine(void *codec, int engine) {
+    wfd::codec::Codec *c = C(codec);
+    if (!c || engine < 0 || engine > 1) return WFD_ERR_ARG;
+    if (engine == 1 && (c->grid_enc_u == 0 || c->grid_dec_u == 0)) return WFD_ERR_UNSUPPORTED;
+    c->engine = engine;
+    return WFD_OK;
+}
+
+extern "C" int WFD_Codec_Engine(void *codec) { return codec ? C(codec)->engine : -1; }
+
+extern "C" int WFD_Codec_Status(void *codec) {
+    if (!codec) return WFD_ERR_ARG;
+    if (cudaDeviceSynchronize() != cudaSuccess) return cuda_status(cudaGetLastError(), "WFD_Codec_Status");
+    unsigned v = 0, z = 0;
+    cudaMemcpyFromSymbol(&v, wfd::codec::d_codec_status, sizeof(v));
+    if (v) {
+        cudaMemcpyToSymbol(wfd::codec::d_codec_status, &z, sizeof(z));
+        wfd::set_global_error(WFD_ERR_TIMEOUT, "codec: a tensor-core completion wait ran out");
+        return WFD_ERR_TIMEOUT;
+    }
+    return WFD_OK;
 }
 
 extern "C" long WFD_Codec_RawBlocks(const void *latent, long nx, long ny, long nz) {
