@@ -583,31 +583,25 @@ def run_born(args, W):
                 "where": f"{tmpdir} (O_DIRECT where the file system allows)"}
     else:
         disk = {"unavailable": f"less than {1.5 * disk_bytes / 1e9:.0f} GB free in {tmpdir}"}
-    # image error at this shape: learned against exact FP32 snapshots kept in device memory, over as
-    # many steps (up to 600) as the device holds the exact snapshots for; the reflectors of this
-    # check lie between 1 % and 10 % of the depth: at 1500 m/s near the surface and with the causal
-    # wavelet's 0.1 s onset, 600 steps of 0.5 ms reach and return from the first six of them
+    # plain FP32 snapshots held on the device by recomputation: checkpoints of the full state every
+    # 200 steps, each segment's snapshots recomputed before the adjoint run crosses it (one forward
+    # pass more); timed over the whole record. Then the image error at this shape over the whole
+    # record: the same checkpointed run with the learned store filled in its forward pass, both images
+    # through one adjoint wavefield (exact snapshots against decoded ones)
     import torch
     del learned
     torch.cuda.empty_cache()
-    snap_bytes = 2 * int(np.prod(W["shape"])) * 4
-    n_img = min(ns, 600)
-    free = torch.cuda.mem_get_info()[0]
-    while n_img > 4 * every and (n_img // every) * snap_bytes > 0.75 * free:
-        n_img -= 4 * every
-    chk = imaging.make_shot("tti", W["shape"], seed=6, d=W["d"], dt=W["dt"], nsponge=W["nsponge"], fpeak=W["fpeak"],
-                            nt=n_img, nrec=W["nrec"], horizons=(0.01, 0.1))
-    chk_data = imaging.born_data(chk)
-    exact_store = imaging.DeviceStore(W["shape"], n_img // every, 2)
-    img_e, _ = imaging.born_image(chk, chk_data, exact_store, every=every)
-    del exact_store
+    seg = 200
+    img_ck, t_ck, _ = imaging.born_image_checkpointed(shot, data, every=every, seg=seg)
+    del img_ck
     torch.cuda.empty_cache()
-    img_l, _ = imaging.born_image(chk, chk_data, imaging.CodecStore(codec, W["shape"], n_img // every, 2),
-                                  every=every)
+    img_e, _, img_l = imaging.born_image_checkpointed(shot, data, every=every, seg=seg,
+                                                      learned=imaging.CodecStore(codec, W["shape"], ns // every, 2))
     ae, al = img_e.double(), img_l.double()
     img_norm = float(torch.linalg.norm(ae))
     rel_full = float(torch.linalg.norm(al - ae) / torch.linalg.norm(ae).clamp_min(1e-30))
     del img_e, img_l, ae, al
+    torch.cuda.empty_cache()
     # image error over a whole record (the sample's first steps image nothing yet): 128^3, 1000 steps
     small = imaging.make_shot("tti", (128, 128, 128), seed=4, d=W["d"], dt=W["dt"], nsponge=20, fpeak=W["fpeak"],
                               nt=1000, nrec=(32, 32))
@@ -639,9 +633,14 @@ def run_born(args, W):
         "image_check": "TTI 128^3, nt 1000, snapshots every 4 steps, learned vs exact FP32 storage",
         "image_rel_l2_at_bench_shape": rel_full,
         "image_l2_norm_at_bench_shape": img_norm,
-        "image_check_at_bench_shape": (f"TTI {'x'.join(map(str, W['shape']))}, a {n_img}-step record with reflectors "
-                                       f"from 1 % to 10 % of the depth, learned vs exact FP32 snapshots in device "
-                                       f"memory"),
+        "image_check_at_bench_shape": (f"TTI {'x'.join(map(str, W['shape']))}, the bench shot's {ns}-step record, "
+                                       f"learned snapshots vs exact FP32 snapshots recomputed from checkpoints every "
+                                       f"{seg} steps, both imaged through one adjoint wavefield"),
+        "plain_checkpointed": {"s_per_shot": round(t_ck * scale, 3), "steps": ns,
+                               "speedup_learned_vs_checkpointed": round(t_ck / t_codec, 3),
+                               "how": (f"exact FP32 snapshots on the device by recomputation: full-state checkpoints "
+                                       f"every {seg} steps, each segment recomputed before the adjoint run crosses "
+                                       f"it (one forward pass more; {seg // every} snapshots resident)")},
         "snapshot_bytes": {"plain": 2 * ncells * 4, "learned": 2 * codec.code_bytes(W["shape"])},
         "codec_training": {"seconds": round(t_train, 2), "blocks": nblocks, "steps": len(hist),
                            "final_loss": float(np.mean(hist[-50:]))},

@@ -327,3 +327,125 @@ def born_image(shot, data, store, every=4, nt=None):
     props.free(fwd)
     props.free(adj)
     return image, secs
+
+
+class _StateArrays:
+    """The two pressure arrays (and two m arrays) of an object, fixed across its pointer swaps, and the
+    object's step count: after n steps pCur is the second array when n is odd, else the first."""
+
+    def __init__(self, prop, shape, aniso):
+        names = [("PCur", "POld")] + ([("MCur", "MOld")] if aniso else [])
+        self.pairs = [(_field(prop, a, shape), _field(prop, b, shape)) for a, b in names]
+        self.n = 0
+
+    def save(self):
+        return [(a.clone(), b.clone()) for a, b in self.pairs], self.n
+
+    def restore(self, saved, stream):
+        """Set the object to the saved state (its pCur/pOld/mCur/mOld values), whatever the parity of
+        the steps taken since: the arrays are exchanged when the parities differ."""
+        import torch
+        arrays, n = saved
+        swap = (self.n - n) & 1
+        with torch.cuda.stream(stream):
+            for (a, b), (sa, sb) in zip(self.pairs, arrays):
+                a.copy_(sb if swap else sa, non_blocking=True)
+                b.copy_(sa if swap else sb, non_blocking=True)
+
+
+def born_image_checkpointed(shot, data, every=4, seg=200, nt=None, learned=None):
+    """Adjoint Born image with exact FP32 forward fields held on the device by recomputation: the
+    forward run keeps the full state (pCur, pOld, mCur, mOld) every `seg` steps; the adjoint run goes
+    through the record segment by segment from the end, recomputing each segment's forward fields
+    from its checkpoint into device memory (seg / every snapshots) before back-propagating over it.
+    One forward pass more than storing every snapshot, for seg / every snapshots of memory instead
+    of nt / every. Returns (image, seconds, learned image or None): with a snapshot store `learned`
+    (filled during the same forward run) the adjoint run also accumulates the image of the learned
+    fields, through the same adjoint wavefield, so that the two images differ only by the stored
+    fields (the timing then includes that second imaging condition)."""
+    import torch
+    shape = shot["shape"]
+    nt = nt or shot["nt"]
+    lib = _lib.library()
+    aniso = shot["physics"] != "iso"
+    linear = shot["physics"] == "vti"
+    fwd, rec, adj = _new_prop(shot), _new_prop(shot), _new_prop(shot)
+    torch.cuda.synchronize()
+    for p in (fwd, rec, adj):
+        p.prefetch()
+    tsrc = lib.WFD_Points_Create(shot["src"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["src"]), 0)
+    tadj = lib.WFD_Points_Create(shot["rec"].ctypes.data_as(ct.POINTER(SourcePoint32)), len(shot["rec"]), 0)
+    image = torch.zeros(shape, device="cuda")
+    image_l = torch.zeros(shape, device="cuda") if learned is not None else None
+    fs, rs, as_ = (torch.cuda.ExternalStream(p.stream()) for p in (fwd, rec, adj))
+    f_space = [_field(fwd, "PSpace", shape)] + ([_field(fwd, "MSpace", shape)] if aniso else [])
+    r_space = [_field(rec, "PSpace", shape)] + ([_field(rec, "MSpace", shape)] if aniso else [])
+    fstate, rstate = _StateArrays(fwd, shape, aniso), _StateArrays(rec, shape, aniso)
+    fcur, rcur, acur = _PCur(fwd), _PCur(rec), _PCur(adj)
+    props.scale_spatial_derivatives(adj)
+    mtype = getattr(props, adj.NAME + "_Model_V")()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fp, rp, ap = ct.c_void_p(fwd.p), ct.c_void_p(rec.p), ct.c_void_p(adj.p)
+    wav = ct.c_void_p(shot["wavelet"].data_ptr())
+
+    def fstep(p, pp, cur, state, it):
+        """forward step `it` of object p with the source injection (the scaled step at saved steps)"""
+        if it % every == 0:
+            _lib.check(lib.WFD_Prop_TimeStepScaled(pp), "scaled step", p.p)
+        else:
+            p.step_async(1)
+        state.n += 1
+        _lib.check(lib.WFD_Inject(tsrc, cur.step(), wav, it, shot["nt"], ct.c_void_p(p.stream())), "inject")
+
+    # forward: checkpoints every seg steps (the state after step k * seg), learned snapshots if any
+    nseg = (nt + seg - 1) // seg
+    checkpoints = []
+    for it in range(1, nt + 1):
+        if (it - 1) % seg == 0:
+            with torch.cuda.stream(fs):
+                checkpoints.append(fstate.save())
+        fstep(fwd, fp, fcur, fstate, it)
+        if learned is not None and it % every == 0:
+            learned.put(it // every - 1, f_space, fs)
+    fwd.synchronize()
+    snaps = {}
+    for s in range(nseg - 1, -1, -1):
+        lo, hi = s * seg + 1, min((s + 1) * seg, nt)
+        # recompute the segment's forward fields from its checkpoint
+        rstate.restore(checkpoints[s], rs)
+        snaps.clear()
+        for it in range(lo, hi + 1):
+            fstep(rec, rp, rcur, rstate, it)
+            if it % every == 0:
+                with torch.cuda.stream(rs):
+                    snaps[it // every - 1] = [t.clone() for t in r_space]
+        rec.synchronize()
+        for it in range(hi, lo - 1, -1):
+            if it % every == 0:
+                k = it // every - 1
+                e = snaps[k]
+                dm = ct.c_void_p(e[1].data_ptr()) if aniso else None
+                _lib.check(lib.WFD_Prop_TimeStepImage(ap, ct.c_void_p(image.data_ptr()), ct.c_void_p(e[0].data_ptr()),
+                                                      dm, int(linear)), "imaging step", adj.p)
+                if learned is not None:
+                    f = learned.get(k, as_)
+                    wf = {"pspace": f[0]}
+                    if aniso:
+                        wf["mspace"] = f[1]
+                    adj.synchronize()
+                    props.adjointBornAccumulation(adj, mtype, props.ImagingConditionStandard(), {"v": image_l}, wf)
+            else:
+                adj.step_async(1, linear=linear)
+            _lib.check(lib.WFD_Inject(tadj, acur.step(), ct.c_void_p(data.data_ptr()), it, shot["nt"],
+                                      ct.c_void_p(adj.stream())), "inject adjoint")
+        adj.synchronize()
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    snaps.clear()
+    del checkpoints
+    lib.WFD_Points_Free(tsrc)
+    lib.WFD_Points_Free(tadj)
+    for p in (fwd, rec, adj):
+        props.free(p)
+    return image, secs, image_l
