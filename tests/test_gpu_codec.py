@@ -98,9 +98,11 @@ def test_encode_decode_matches_oracle(torch, engine):
 
 def test_tcgen05_engine_matches_mma_sync(torch):
     """The tcgen05 kernels (UMMA, accumulators in tensor memory) against the mma.sync ones on the same
-    weights and field: the same BF16 roundings, so the codes agree up to a rare last-bit difference
-    (a sum formed in another order rounds to the neighbouring BF16 value) and the decoded fields agree
-    to BF16 accuracy; a grid with partial slabs in every direction."""
+    weights and field, a grid with partial slabs in every direction. Decoding the same codes with the
+    two engines agrees to FP32 accumulation order; encoding agrees to the last BF16 bit of a few codes,
+    so the two round trips agree to BF16 accuracy on the blocks that neither engine keeps raw (which
+    blocks of the lowest selected error bin are kept raw may differ: their error energies are sums
+    formed in another order)."""
     from wavefd_b200.codec import WavefieldCodec
     codec = WavefieldCodec(seed=9)
     assert codec.engine == "tcgen05"
@@ -110,27 +112,33 @@ def test_tcgen05_engine_matches_mma_sync(torch):
     for ax in range(3):
         for _ in range(2):
             f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
-    d_f = torch.from_numpy(f.astype(np.float32)).cuda()
-    outs, codes = {}, {}
+    f = f.astype(np.float32)
+    d_f = torch.from_numpy(f).cuda()
+    codes = {}
     for engine in ("tcgen05", "mma.sync"):
         codec.engine = engine
-        code = codec.empty_code(shape)
-        out = torch.empty(shape, device="cuda")
-        codec.encode(d_f, shape, code)
-        codec.decode(code, shape, out)
+        codes[engine] = codec.empty_code(shape)
+        codec.encode(d_f, shape, codes[engine])
         codec.status()
-        outs[engine], codes[engine] = out.double(), code.clone()
-    a, b = outs["tcgen05"], outs["mma.sync"]
-    rel = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-    assert rel <= 5e-3, rel
-    for o in outs.values():
-        assert bool(torch.isfinite(o).all())
-    # cross decoding: codes of one engine decoded by the other
-    codec.engine = "mma.sync"
-    cross = torch.empty(shape, device="cuda")
-    codec.decode(codes["tcgen05"], shape, cross)
-    codec.status()
-    assert float(torch.linalg.norm(cross.double() - a) / torch.linalg.norm(a)) <= 5e-3
+    dec = {}
+    for ce in ("tcgen05", "mma.sync"):
+        for de in ("tcgen05", "mma.sync"):
+            codec.engine = de
+            out = torch.empty(shape, device="cuda")
+            codec.decode(codes[ce], shape, out)
+            codec.status()
+            dec[ce, de] = out.cpu().numpy().astype(np.float64)
+    for ce in ("tcgen05", "mma.sync"):
+        a, b = dec[ce, "tcgen05"], dec[ce, "mma.sync"]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel <= 1e-5, (ce, rel)
+    B0, _ = co.blocks_of(f)
+    Ba, _ = co.blocks_of(dec["tcgen05", "tcgen05"].astype(np.float32))
+    Bb, _ = co.blocks_of(dec["mma.sync", "mma.sync"].astype(np.float32))
+    raw_a, raw_b = np.all(Ba == B0, axis=1), np.all(Bb == B0, axis=1)
+    keep = ~raw_a & ~raw_b
+    rel = np.linalg.norm(Ba[keep] - Bb[keep]) / np.linalg.norm(Bb[keep])
+    assert rel <= 5e-3, (rel, int(raw_a.sum()), int(raw_b.sum()), int((raw_a & raw_b).sum()))
 
 
 def test_training_reduces_loss(trained):

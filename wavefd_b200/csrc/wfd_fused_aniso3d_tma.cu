@@ -465,6 +465,21 @@ __global__ void __launch_bounds__(NT, 1)
                     m_issued++;
                 }
             }
+            // the epilogue's inputs of plane j, loaded now so that their latency hides behind the waits
+            // and pass 1 (born: dV, DP, DM; imaging: the image, DP, DM)
+            float2 ea = bc2(0.0f), eb = bc2(0.0f), ec = bc2(0.0f);
+            if (EPI && own && j >= xbeg) {
+                const long k = j * g.sx + (long)y * g.nz + z;
+                if (F.epi.born_dv) {
+                    ea = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dv + k));
+                    eb = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dp + k));
+                    ec = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dm + k));
+                } else if (F.epi.img) {
+                    ea = ld2(F.epi.img + k);
+                    eb = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dp + k));
+                    ec = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dm + k));
+                }
+            }
             bool ok_w = true;
             if (q >= 1 && q + 7 < nplanes) {
                 const unsigned gi = rseq + q + 7;
@@ -560,7 +575,7 @@ __global__ void __launch_bounds__(NT, 1)
                 // Born-V injection fused after the step (prop3DAcoTTIDenQ_DEO2_FDTD.h:423-452):
                 // new += 2 dt^2 dV/V * DP (DM), every cell
                 float2 bfac = bc2(0.0f);
-                if (EPI && F.epi.born_dv) bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), ld2(F.epi.born_dv + k)), V);
+                if (EPI && F.epi.born_dv) bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), ea), V);
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
                     const float2 pc = ld2(ring[0] + f * RBOX + ro);
@@ -568,7 +583,7 @@ __global__ void __launch_bounds__(NT, 1)
                     const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc, po))), po);
                     const float2 np = add2(t, mul2(bc2(2.0f), pc));
                     float2 nv = ok ? np : po;
-                    if (EPI && F.epi.born_dv) nv = add2(nv, mul2(bfac, ld2((f == 0 ? F.epi.born_dp : F.epi.born_dm) + k)));
+                    if (EPI && F.epi.born_dv) nv = add2(nv, mul2(bfac, f == 0 ? eb : ec));
                     st2((f == 0 ? out_pold : out_mold) + k, nv);
                     if (!LINEAR) {
                         float2 sp = ok ? L[f] : bc2(0.0f);
@@ -582,9 +597,7 @@ __global__ void __launch_bounds__(NT, 1)
                     // mOld), pOld/mOld being this step's input pCur/mCur
                     const float2 pcp = ld2(ring[0] + ro), pcm = ld2(ring[0] + RBOX + ro);
                     const float2 fac = div2(mul2(bc2(2.0f), B), mul2(mul2(V, V), V));
-                    float2 a = ld2(F.epi.img + k);
-                    a = add2(a, mul2(fac, add2(mul2(ld2(F.epi.img_dp + k), pcp), mul2(ld2(F.epi.img_dm + k), pcm))));
-                    st2(F.epi.img + k, a);
+                    st2(F.epi.img + k, add2(ea, mul2(fac, add2(mul2(eb, pcp), mul2(ec, pcm)))));
                 }
                 if (!BATCH && F.illum) {
                     // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add,

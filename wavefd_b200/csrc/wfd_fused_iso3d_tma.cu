@@ -225,7 +225,7 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
                                           const int y, const unsigned fmask, const int zq, const int row,
                                           const float2 *sx, const float2 *pc, const float *st, const float *TYs,
                                           const float *TZs, float *po, float *ps, float *illum,
-                                          const StepEpilogue *epi) {
+                                          const StepEpilogue *epi, const float4 ea, const float4 eb) {
     const int o = row * TZ + 4 * zq;
     const float4 pold4 = ld4(st + S_PO + o), v4 = ld4(st + S_V + o), q4 = ld4(st + S_Q + o);
     const float4 b4 = ld4(st + S_BH + (4 + row) * BZW + 4 + 4 * zq);
@@ -286,18 +286,17 @@ __device__ __forceinline__ void fin_stage(const Grid &g, const long j, const boo
             nl = mul2(nl, div2(mul2(V, V), half2(b4, h)));
         if (EPI && epi->born_dv) {
             // Born-V injection fused after the step (prop3DAcoIsoDenQ_DEO2_FDTD.h:305-334), every cell:
-            // new += dt^2 V^2/B * DP * (2 B dV / V^3)
-            const long kc = j * g.sx + (long)y * g.nz + z + m0;
+            // new += dt^2 V^2/B * DP * (2 B dV / V^3); ea = dV, eb = DP (loaded early)
             const float2 B = half2(b4, h);
-            const float2 fv = div2(mul2(mul2(bc2(2.0f), B), ld2(epi->born_dv + kc)), mul2(mul2(V, V), V));
-            np = add2(np, mul2(mul2(k2, ld2(epi->born_dp + kc)), fv));
+            const float2 fv = div2(mul2(mul2(bc2(2.0f), B), half2(ea, h)), mul2(mul2(V, V), V));
+            np = add2(np, mul2(mul2(k2, half2(eb, h)), fv));
         }
         if (EPI && epi->img) {
             // imaging condition fused after the step (.h:518-546): img += 2B/V^3 DP pOld, pOld being
-            // this step's input pCur
+            // this step's input pCur; ea = the image, eb = DP (loaded early)
             const long kc = j * g.sx + (long)y * g.nz + z + m0;
             const float2 fv = div2(mul2(bc2(2.0f), half2(b4, h)), mul2(mul2(V, V), V));
-            st2(epi->img + kc, add2(ld2(epi->img + kc), mul2(mul2(fv, ld2(epi->img_dp + kc)), pcv)));
+            st2(epi->img + kc, add2(half2(ea, h), mul2(mul2(fv, half2(eb, h)), pcv)));
         }
         npo[h] = np;
         nps[h] = nl;
@@ -468,6 +467,19 @@ __global__ void __launch_bounds__(NT, 3)
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
             }
+            // the epilogue's inputs of plane j, loaded now so that their latency hides behind the wait
+            // and the queue work (born: dV, DP; imaging: the image, DP)
+            float4 ea = make_float4(0.0f, 0.0f, 0.0f, 0.0f), eb = ea;
+            if (EPI && own && j >= xbeg) {
+                const long k = j * g.sx + (long)y * g.nz + z;
+                if (F.epi.born_dv) {
+                    ea = __ldg(reinterpret_cast<const float4 *>(F.epi.born_dv + k));
+                    eb = __ldg(reinterpret_cast<const float4 *>(F.epi.born_dp + k));
+                } else if (F.epi.img) {
+                    ea = ld4(F.epi.img + k);
+                    eb = __ldg(reinterpret_cast<const float4 *>(F.epi.img_dp + k));
+                }
+            }
             const bool landed = mbar_wait(&bars[slot], par);
             if (!landed) {
                 atomicExch(abort_flag, 1);
@@ -501,7 +513,7 @@ __global__ void __launch_bounds__(NT, 3)
                 ext_stage<EDGE>(g, xin, tile_top, z0, emask, st, TYs, TZs);
                 __syncthreads();
                 if (own) fin_stage<EDGE, EPI>(g, j, xin, tile_top, z, y, fmask, zq, row, sx, pc, st, TYs, TZs, out_pold,
-                                               out_pspace, BATCH ? nullptr : F.illum, EPI ? &F.epi : nullptr);
+                                               out_pspace, BATCH ? nullptr : F.illum, EPI ? &F.epi : nullptr, ea, eb);
             }
             __syncthreads();
             if (*abort_flag) {

@@ -392,6 +392,21 @@ __global__ void __launch_bounds__(NT, 2)
                 issue(j + D, gs + D);
                 out_to = gs + D + 1;
             }
+            // the epilogue's inputs of plane j, loaded now so that their latency hides behind the wait
+            // and the pass-1 work (born: dV, DP, DM; imaging: the image, DP, DM)
+            float2 ea = bc2(0.0f), eb = bc2(0.0f), ec = bc2(0.0f);
+            if (EPI && own && j >= xbeg) {
+                const long k = j * g.sx + (long)y * g.nz + z;
+                if (F.epi.born_dv) {
+                    ea = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dv + k));
+                    eb = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dp + k));
+                    ec = __ldg(reinterpret_cast<const float2 *>(F.epi.born_dm + k));
+                } else if (F.epi.img) {
+                    ea = ld2(F.epi.img + k);
+                    eb = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dp + k));
+                    ec = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dm + k));
+                }
+            }
             const bool landed = mbar_wait(&bars[gs % NS], (gs / NS) & 1u);
             if (!landed) {
                 atomicExch(abort_flag, 1);
@@ -462,18 +477,14 @@ __global__ void __launch_bounds__(NT, 2)
                     // Born-V injection fused after the step (prop3DAcoVTIDenQ_DEO2_FDTD.h:420-452):
                     // new += 2 dt^2 dV/V * DP (DM), every cell
                     float2 bfac = bc2(0.0f);
-                    if (EPI && F.epi.born_dv)
-                        bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), __ldg(reinterpret_cast<const float2 *>(F.epi.born_dv + k))), V);
+                    if (EPI && F.epi.born_dv) bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), ea), V);
 #pragma unroll
                     for (int f = 0; f < 2; f++) {
                         const float2 po = ld2(st + (f == 0 ? S_PO : S_MO) + o);
                         const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc[f], po))), po);
                         const float2 np = add2(t, mul2(bc2(2.0f), pc[f]));
                         float2 nv = make_float2(ok0 ? np.x : po.x, ok1 ? np.y : po.y);
-                        if (EPI && F.epi.born_dv) {
-                            const float *d = f == 0 ? F.epi.born_dp : F.epi.born_dm;
-                            nv = add2(nv, mul2(bfac, __ldg(reinterpret_cast<const float2 *>(d + k))));
-                        }
+                        if (EPI && F.epi.born_dv) nv = add2(nv, mul2(bfac, f == 0 ? eb : ec));
                         st2((f == 0 ? o_po : o_mo) + k, nv);
                         if (!LINEAR) {
                             float2 sp = make_float2(ok0 ? L[f].x : 0.0f, ok1 ? L[f].y : 0.0f);
@@ -485,12 +496,8 @@ __global__ void __launch_bounds__(NT, 2)
                     if (EPI && F.epi.img) {
                         // imaging condition fused after the step (.h:564-589): img += 2B/V^3 (DP pOld +
                         // DM mOld), pOld/mOld being this step's input pCur/mCur
-                        const float2 dp = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dp + k));
-                        const float2 dm = __ldg(reinterpret_cast<const float2 *>(F.epi.img_dm + k));
                         const float2 fac = div2(mul2(bc2(2.0f), B), mul2(mul2(V, V), V));
-                        float2 a = ld2(F.epi.img + k);
-                        a = add2(a, mul2(fac, add2(mul2(dp, pc[0]), mul2(dm, pc[1]))));
-                        st2(F.epi.img + k, a);
+                        st2(F.epi.img + k, add2(ea, mul2(fac, add2(mul2(eb, pc[0]), mul2(ec, pc[1])))));
                     }
                     if (!BATCH && F.illum) {
                         // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and

@@ -315,6 +315,13 @@ int prop_sync(Prop *p) {
 int prop_step(Prop *p, bool linear, bool sync) {
     Grid g = p->grid();
     Fields F = p->fields();
+    // the step kernels read the epilogue's arrays 16 (Iso) or 8 bytes at a time: arrays at other
+    // alignments take the separate kernels after the step
+    auto a16 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    const StepEpilogue &pe = p->epi;
+    if (!(a16(pe.born_dv) && a16(pe.born_dp) && a16(pe.born_dm) && a16(pe.img) && a16(pe.img_dp) &&
+          a16(pe.img_dm)))
+        F.epi = StepEpilogue{};
     bool done = false, illum_done = false, epi_done = false;
     p->inject_done = false;
     if (p->fused) {
