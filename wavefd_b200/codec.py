@@ -117,7 +117,7 @@ class WavefieldCodec:
 
     @property
     def engine(self) -> str:
-        """"tcgen05" (UMMA with the accumulators in tensor memory, the default) or "mma.sync"."""
+        """"mma.sync" (the default) or "tcgen05" (UMMA with the accumulators in tensor memory)."""
         return "tcgen05" if _L().WFD_Codec_Engine(self.c) == 1 else "mma.sync"
 
     @engine.setter
