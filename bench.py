@@ -81,8 +81,9 @@ WORKLOADS = {
     # FP32 storage in pinned host memory; a sample of the time loop, scaled to the full record
     "born512": dict(physics="tti", name="born", shape=(512, 512, 400), d=10.0, dt=0.0005, nt=3000, every=4,
                     nsponge=40, fpeak=12.0, nrec=(64, 64),
-                    label="batched 3D TTI DenQ Born imaging, 512x512x400, nt 3000, snapshots every 4 steps: "
-                          "learned BF16 autoencoder compression vs plain FP32 storage (pinned host memory)"),
+                    label="3D TTI DenQ Born imaging of one shot of the 16-shot job's shape, 512x512x400, nt 3000, "
+                          "snapshots every 4 steps: learned BF16 autoencoder compression vs plain FP32 storage "
+                          "(pinned host memory; checkpointed recomputation on the device; disk)"),
 }
 METRIC = "Mcells/s & %HBM roofline, 3D Iso/TTI step; Born image s/shot learned vs plain"
 
