@@ -340,3 +340,56 @@ def test_illumination_fused_into_step(lib, name, shape):
     assert np.array_equal(acc.cpu().numpy(), want)
     assert lib.WFD_Prop_SetIllumination(ctypes.c_void_p(g.p), None) == 0
     g.close()
+
+
+@pytest.mark.parametrize("spread", ["local", "far"])
+def test_prop_run_2d_tiles(lib, spread):
+    """The 2D Iso whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each):
+    receiver groups whose cells lie in one tile's neighbourhood run the neighbour-synchronised kernel
+    (each group extracted by its tile), a group spanning farther takes the grid-wide barrier version.
+    Both against TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build)."""
+    import torch
+    from tests.harness import ABIRunner, make_model
+    name, shape = "Prop2DAcoIsoDenQ_DEO2_FDTD", (200, 1, 90)  # nz 200 (4 tiles), nx 90 (6 tiles)
+    nz, ny, nx = shape
+    nt, nsteps = 40, 17
+    gap = nz * (1 if spread == "local" else 40)  # the second point of a group: 1 or 40 rows further in x
+    pts = []
+    for i in range(12):
+        k = (5 + 6 * i) * nz + 7 + 13 * i
+        pts.append(SourcePoint32(k + 1, i + 1, 0.6))
+        pts.append(SourcePoint32(min(k + gap, nz * nx - 1) + 1, i + 1, 0.4))
+    runs = []
+    for mode in ("run", "steps"):
+        g = ABIRunner(lib, name, shape, fs=True)
+        lib.WFD_Prop_SetStrict(ctypes.c_void_p(g.p), 1)
+        g.load(make_model(2, "iso", shape, seed=8))
+        src = (SourcePoint32 * 1)(SourcePoint32((nx // 2) * nz + 3, 1, 1.0))
+        ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), 1, 0)
+        rec = (SourcePoint32 * len(pts))(*pts)
+        tr = lib.WFD_Points_Create(ctypes.cast(rec, ctypes.POINTER(SourcePoint32)), len(pts), 1)
+        wav = torch.from_numpy(np.random.default_rng(3).standard_normal(nt).astype(np.float32)).cuda()
+        trc = torch.zeros(12 * nt, device="cuda")
+        torch.cuda.synchronize()
+        stream = ctypes.c_void_p(lib.WFD_Prop_Stream(ctypes.c_void_p(g.p)))
+        if mode == "run":
+            assert lib.WFD_Prop_Run(ctypes.c_void_p(g.p), nsteps, 1, ts, ctypes.c_void_p(wav.data_ptr()), tr,
+                                    ctypes.c_void_p(trc.data_ptr()), nt, 1) == 0
+            assert lib.WFD_Prop_RunLaunches(ctypes.c_void_p(g.p)) == 1
+        else:
+            for it in range(1, 1 + nsteps):
+                assert lib.WFD_Prop_TimeStepAsync(ctypes.c_void_p(g.p), 1, 0) == 0
+                pc = ctypes.c_void_p(ctypes.cast(g.abi.getPCur(g.p), ctypes.c_void_p).value)
+                assert lib.WFD_Inject(ts, pc, ctypes.c_void_p(wav.data_ptr()), it, nt, stream) == 0
+                assert lib.WFD_Extract(tr, ctypes.c_void_p(trc.data_ptr()), pc, it, nt, stream) == 0
+        assert lib.WFD_Prop_Synchronize(ctypes.c_void_p(g.p)) == 0
+        assert lib.WFD_Prop_Status(ctypes.c_void_p(g.p)) == 0
+        runs.append(({k: g.arr(k).copy() for k in ("PCur", "POld", "PSpace")}, trc.cpu().numpy()))
+        lib.WFD_Points_Free(ts)
+        lib.WFD_Points_Free(tr)
+        g.close()
+    (fa, ta), (fb, tb) = runs
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), (k, mismatch_report(fa[k], fb[k]))
+    assert np.array_equal(ta, tb)
+    assert np.count_nonzero(ta) > 0
