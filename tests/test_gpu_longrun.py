@@ -176,3 +176,43 @@ def test_whole_record_parity(lib, oracle, key, strict):
     c = CASES[key]
     _report({"case": key, "build": "strict" if strict else "fast", "grid": [c["nx"], c["ny"], c["nz"]],
              "nt": c["nt"], "errors": errs})
+
+
+@pytest.mark.parametrize("strict", [True, False])
+def test_whole_record_prop_run_2d(lib, oracle, strict):
+    """Config 0 whole through the whole-loop launch (WFD_Prop_Run: 2000 steps, injection and
+    extraction inside one cooperative kernel with neighbour-only synchronisation between tiles)
+    against the FP32 restatement: bitwise in the strict build, within the fast bound otherwise."""
+    import torch
+    from wavefd_b200.abi import SourcePoint32
+    key = "iso2d_501"
+    f32, tr32, f64, tr64, model, src, rec, wav = _oracle_run(oracle, key)
+    c = CASES[key]
+    shape = (c["nz"], c["ny"], c["nx"])
+    gpu = ABIRunner(lib, c["name"], shape, fs=True, nsponge=c["nsponge"], dx=c["d"], dt=c["dt"])
+    lib.WFD_Prop_SetStrict(ctypes.c_void_p(gpu.p), int(strict))
+    gpu.load(model)
+    nt = c["nt"]
+    ts = lib.WFD_Points_Create(src.ctypes.data_as(ctypes.POINTER(SourcePoint32)), len(src), 0)
+    tr = lib.WFD_Points_Create(rec.ctypes.data_as(ctypes.POINTER(SourcePoint32)), len(rec), 1)
+    d_wav = torch.from_numpy(np.ascontiguousarray(wav, np.float32)).cuda()
+    d_tr = torch.zeros(len(rec) * nt, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.WFD_Prop_Run(ctypes.c_void_p(gpu.p), nt, 1, ts, ctypes.c_void_p(d_wav.data_ptr()), tr,
+                            ctypes.c_void_p(d_tr.data_ptr()), nt, 1) == 0
+    assert lib.WFD_Prop_Synchronize(ctypes.c_void_p(gpu.p)) == 0
+    assert lib.WFD_Prop_RunLaunches(ctypes.c_void_p(gpu.p)) == 1
+    g = {k: gpu.arr(k).copy() for k in _fields(c["physics"])}
+    trg = d_tr.cpu().numpy()
+    lib.WFD_Points_Free(ts)
+    lib.WFD_Points_Free(tr)
+    gpu.close()
+    for k in f32:
+        if strict:
+            assert np.array_equal(g[k], f32[k]), f"{k}: rel L2 {rel_l2(g[k], f32[k]):.3e}"
+        else:
+            assert rel_l2(g[k], f32[k]) <= max(FAST_TOL, 2 * rel_l2(f32[k], f64[k]))
+    if strict:
+        assert np.array_equal(trg, tr32)
+    else:
+        assert rel_l2(trg, tr32) <= max(FAST_TOL, 2 * rel_l2(tr32, tr64))
