@@ -362,8 +362,9 @@ __global__ void __launch_bounds__(NT) k_iso2d_run_nbr(Grid g, Fields F, long nst
         Fs.pcur = (st & 1) ? B : A;
         Fs.pold = (st & 1) ? A : B;
         if (st > 0) {
+            // the polling threads' acquire loads, then the CTA barrier inside the wait, order every
+            // thread's later reads (past L1) after the neighbours' writes
             if (!wait_tiles(flags, nbr, nn, (unsigned)st, status)) return;
-            __threadfence();
             extract(st - 1);
         }
         tile_step(g, Fs, (long)txi * TX, (long)tzi * TZ, it0 + st, sm);
@@ -373,10 +374,7 @@ __global__ void __launch_bounds__(NT) k_iso2d_run_nbr(Grid g, Fields F, long nst
             asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flags + t), "r"((unsigned)(st + 1)) : "memory");
         }
     }
-    if (nsteps > 0 && wait_tiles(flags, nbr, nn, (unsigned)nsteps, status)) {
-        __threadfence();
-        extract(nsteps - 1);
-    }
+    if (nsteps > 0 && wait_tiles(flags, nbr, nn, (unsigned)nsteps, status)) extract(nsteps - 1);
 }
 }  // namespace
 

@@ -437,7 +437,9 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     const long ntz = (p->nz + wfd::ISO2D_TILE_Z - 1) / wfd::ISO2D_TILE_Z;
     const long ntiles = ntz * ((p->nx + wfd::ISO2D_TILE_X - 1) / wfd::ISO2D_TILE_X);
     std::vector<int> tstart, tgroups;
-    bool by_tiles = run2d && ntiles < (1L << 20);
+    // WAVEFD_B200_RUN2D=barrier keeps the grid-wide barrier version (for comparisons)
+    const char *run_mode = getenv("WAVEFD_B200_RUN2D");
+    bool by_tiles = run2d && ntiles < (1L << 20) && !(run_mode && strcmp(run_mode, "barrier") == 0);
     if (by_tiles && rec && rec->t.ngroups) {
         const auto &t = rec->t;
         std::vector<long> owner(t.ngroups);
