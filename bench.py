@@ -519,7 +519,7 @@ def run_codec(args, W):
                                                               "l2": "L2 flushed (256 MB write) before each launch"},
         "code_bytes": cb, "compression_ratio_bytes": round(4 * n / cb, 2),
         "encode": head["encode"], "decode": head["decode"], "field_rel_l2": head["field_rel_l2"],
-        "engines": {"tcgen05": umma, "mma.sync": legacy},
+        "engines": {"tcgen05": umma, "mma.sync": legacy}, "grids": codec.grids(),
         "roofline": {"bound": "hbm", "achieved": round(ach_e, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach_e / peak, 4), "traffic": None,
                      "kernel": "k_encode (mma.sync, the default engine; + raw-block selection)",

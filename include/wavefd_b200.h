@@ -452,6 +452,8 @@ int WFD_Codec_Decode(void *codec, const void *latent, long nx, long ny, long nz,
  * tcgen05 kernels cannot be launched here. WAVEFD_B200_CODEC=tcgen05 selects engine 1 at creation. */
 int WFD_Codec_SetEngine(void *codec, int engine);
 int WFD_Codec_Engine(void *codec);
+/* CTAs launched by the encode (0: mma.sync, 2: tcgen05) and decode (1: mma.sync, 3: tcgen05) kernels */
+int WFD_Codec_Grid(void *codec, int kernel);
 /* Synchronises the device; WFD_ERR_TIMEOUT (and clears it) when a tcgen05 completion wait of an
  * encode or decode ran out (bounded at 2 s), else WFD_OK. */
 int WFD_Codec_Status(void *codec);

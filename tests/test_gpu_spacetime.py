@@ -344,10 +344,9 @@ def test_illumination_fused_into_step(lib, name, shape):
 
 @pytest.mark.parametrize("spread", ["local", "far"])
 def test_prop_run_2d_tiles(lib, spread):
-    """The 2D Iso whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each):
-    receiver groups whose cells lie in one tile's neighbourhood run the neighbour-synchronised kernel
-    (each group extracted by its tile), a group spanning farther takes the grid-wide barrier version.
-    Both against TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build)."""
+    """The 2D Iso whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each),
+    receiver groups of two points one row apart or 40 rows apart (more than two tiles), against
+    TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build)."""
     import torch
     from tests.harness import ABIRunner, make_model
     name, shape = "Prop2DAcoIsoDenQ_DEO2_FDTD", (200, 1, 90)  # nz 200 (4 tiles), nx 90 (6 tiles)

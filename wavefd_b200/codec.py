@@ -45,6 +45,7 @@ def _L():
         fn("WFD_Codec_RawBlocks", c_long, [c_void_p, c_long, c_long, c_long])
         fn("WFD_Codec_SetEngine", c_int, [c_void_p, c_int])
         fn("WFD_Codec_Engine", c_int, [c_void_p])
+        fn("WFD_Codec_Grid", c_int, [c_void_p, c_int])
         fn("WFD_Codec_Status", c_int, [c_void_p])
         fn("WFD_Codec_GatherBlocks", c_int, [c_void_p, c_long, c_long, c_long, c_void_p, c_long, c_void_p, c_void_p,
                                              c_void_p])
@@ -123,6 +124,11 @@ class WavefieldCodec:
     @engine.setter
     def engine(self, name: str):
         _check(_L().WFD_Codec_SetEngine(self.c, {"tcgen05": 1, "mma.sync": 0}[name]), "SetEngine")
+
+    def grids(self):
+        """CTAs launched by each coding kernel."""
+        names = ("encode mma.sync", "decode mma.sync", "encode tcgen05", "decode tcgen05")
+        return {n: int(_L().WFD_Codec_Grid(self.c, i)) for i, n in enumerate(names)}
 
     def status(self):
         """Synchronises the device; raises if a tensor-core completion wait ran out."""

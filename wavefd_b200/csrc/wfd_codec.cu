@@ -913,6 +913,28 @@ extern "C" void *WFD_Codec_Create(unsigned seed) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&peu, k_encode_umma, NTC, umma_layout::E_BYTES) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pdu, k_decode_umma, NTC, umma_layout::D_BYTES) == cudaSuccess &&
         peu > 0 && pdu > 0;
+    // CTAs per SM from the kernels' own resource use (shared memory, registers, and 64 of the 512
+    // tensor-memory columns each), where that exceeds the occupancy query's answer (which returned 1
+    // per SM for these kernels on a B200 where ncu reports 4 decode CTAs fitting); a grid larger than
+    // what fits only runs in more waves, the CTAs never wait on one another
+    auto fit = [&](const void *kern, int bytes) {
+        cudaFuncAttributes a{};
+        int smem_sm = 0, regs_sm = 0;
+        if (cudaFuncGetAttributes(&a, kern) != cudaSuccess) return 1;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, c->device);
+        const int by_smem = smem_sm / (bytes + (int)a.sharedSizeBytes + 1024);
+        const int by_regs = a.numRegs > 0 ? regs_sm / (a.numRegs * NTC) : 1;
+        int n = by_smem < by_regs ? by_smem : by_regs;
+        n = n < 512 / umma_layout::TMEM_COLS ? n : 512 / umma_layout::TMEM_COLS;
+        return n > 0 ? n : 1;
+    };
+    if (umma_ok) {
+        const int fe = fit((const void *)k_encode_umma, umma_layout::E_BYTES);
+        const int fd = fit((const void *)k_decode_umma, umma_layout::D_BYTES);
+        peu = peu > fe ? peu : fe;
+        pdu = pdu > fd ? pdu : fd;
+    }
     c->grid_enc_u = umma_ok ? sms * (peu < 8 ? peu : 8) : 0;
     c->grid_dec_u = umma_ok ? sms * (pdu < 8 ? pdu : 8) : 0;
     // default: mma.sync, measured faster at 512x512x400 (encode 0.28 against 0.48 ms, decode 0.16
@@ -1021,6 +1043,18 @@ extern "C" int WFD_Codec_SetEngine(void *codec, int engine) {
 }
 
 extern "C" int WFD_Codec_Engine(void *codec) { return codec ? C(codec)->engine : -1; }
+
+extern "C" int WFD_Codec_Grid(void *codec, int kernel) {
+    if (!codec) return -1;
+    const wfd::codec::Codec *c = C(codec);
+    switch (kernel) {
+        case 0: return c->grid_enc;
+        case 1: return c->grid_dec;
+        case 2: return c->grid_enc_u;
+        case 3: return c->grid_dec_u;
+        default: return -1;
+    }
+}
 
 extern "C" int WFD_Codec_Status(void *codec) {
     if (!codec) return WFD_ERR_ARG;

@@ -20,7 +20,7 @@ using namespace wfd;
 
 namespace {
 
-constexpr int TX = ISO2D_TILE_X, TZ = ISO2D_TILE_Z, NT = 512;
+constexpr int TX = 16, TZ = 64, NT = 512;
 constexpr int PXH = TX + 14, PZW = TZ + 14;  // pCur box: rows x0-7 .., columns z0-7 ..
 constexpr int BXH = TX + 8, BZW = TZ + 8;    // B box: rows x0-4 .., columns z0-4 ..
 constexpr int T0H = TX + 7;                  // pass-1 x output: rows x0-4 .. x0+TX+2, columns z0 ..
@@ -83,7 +83,7 @@ __device__ __forceinline__ void tile_step(const Grid &g, const Fields &F, const 
     }
 
     // pCur with its antisymmetric image above kz = 0 (zero outside the grid elsewhere); read past L1
-    // (in a whole-loop launch the neighbouring tiles rewrite it between steps)
+    // (in the whole-loop launch other CTAs rewrite it between steps)
 #pragma unroll
     for (int r = tx; r < PXH; r += WX) {
         const long x = x0 - 7 + r;
@@ -284,130 +284,22 @@ __global__ void __launch_bounds__(NT) k_iso2d_run(Grid g, Fields F, long nsteps,
         }
     }
 }
-// Waits (bounded, 2 s) until every listed tile has finished `target` steps: flag[t] counts the steps a
-// tile has finished in this launch. One thread per neighbour polls with acquire loads; false, for the
-// whole CTA, when a wait ran out or another CTA reported one (status word).
-__device__ __forceinline__ bool wait_tiles(const unsigned *flags, const int *nbr, int nn, unsigned target,
-                                           unsigned *status) {
-    int bad = 0;
-    if (threadIdx.x < nn) {
-        const unsigned *f = flags + nbr[threadIdx.x];
-        uint64_t t0;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-        for (;;) {
-            unsigned v;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
-            if (v >= target) break;
-            if (*(volatile unsigned *)status) {
-                bad = 1;
-                break;
-            }
-            uint64_t t;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-            if (t - t0 > 2000000000ull) {
-                atomicOr(status, 1u);
-                bad = 1;
-                break;
-            }
-            __nanosleep(32);
-        }
-    }
-    return __syncthreads_or(bad) == 0;
-}
-
-// The whole time loop with neighbour-only synchronisation: one CTA per tile (all co-resident:
-// cooperative launch), and before step s a tile waits only until its (up to 8) neighbouring tiles
-// have finished step s-1, instead of a grid-wide barrier. That suffices: step s reads the pCur halo
-// from the neighbours (their step s-1 output) and overwrites the array the neighbours read as pCur
-// in step s-1; a tile's cells are written by that tile only. The receiver groups are split over the
-// tiles (tile t extracts the groups listed in tgroups[tstart[t] .. tstart[t+1]), each group's cells
-// lying in t or its neighbours); tile t extracts step s-1 after its wait, before its step s, which
-// is also before any neighbour can start step s+1 (the next write of that array).
-__global__ void __launch_bounds__(NT) k_iso2d_run_nbr(Grid g, Fields F, long nsteps, long it0, RunExtract ex,
-                                                      unsigned *status, unsigned *flags, const int *tstart,
-                                                      const int *tgroups) {
-    __shared__ Tile sm;
-    __shared__ int nbr[8];
-    __shared__ int nn;
-    const int ntz = (int)((g.nz + TZ - 1) / TZ), ntx = (int)((g.nx + TX - 1) / TX);
-    const int t = blockIdx.x, tzi = t % ntz, txi = t / ntz;
-    if (threadIdx.x == 0) {
-        int n = 0;
-        for (int dx = -1; dx <= 1; dx++)
-            for (int dz = -1; dz <= 1; dz++) {
-                const int a = txi + dx, b = tzi + dz;
-                if ((dx || dz) && a >= 0 && a < ntx && b >= 0 && b < ntz) nbr[n++] = a * ntz + b;
-            }
-        nn = n;
-    }
-    __syncthreads();
-    float *A = F.pcur, *B = F.pold;
-    auto extract = [&](long st) {
-        // the groups of this tile, from the new field of step st (each group in order, IEEE
-        // multiply and add, as the extraction kernel does)
-        const long it = it0 + st;
-        if (!ex.ngroups || it < 1 || it > ex.nt) return;
-        const float *nf = (st & 1) ? A : B;
-        for (int q = tstart[t] + (int)threadIdx.x; q < tstart[t + 1]; q += NT) {
-            const long gi = tgroups[q];
-            float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
-            float acc = *dst;
-            for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
-                acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(nf + ex.other[j])));
-            *dst = acc;
-        }
-    };
-    for (long st = 0; st < nsteps; st++) {
-        Fields Fs = F;
-        Fs.pcur = (st & 1) ? B : A;
-        Fs.pold = (st & 1) ? A : B;
-        if (st > 0) {
-            // the polling threads' acquire loads, then the CTA barrier inside the wait, order every
-            // thread's later reads (past L1) after the neighbours' writes
-            if (!wait_tiles(flags, nbr, nn, (unsigned)st, status)) return;
-            extract(st - 1);
-        }
-        tile_step(g, Fs, (long)txi * TX, (long)tzi * TZ, it0 + st, sm);
-        __syncthreads();  // every thread's stores of this step are issued
-        if (threadIdx.x == 0) {
-            __threadfence();
-            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flags + t), "r"((unsigned)(st + 1)) : "memory");
-        }
-    }
-    if (nsteps > 0 && wait_tiles(flags, nbr, nn, (unsigned)nsteps, status)) extract(nsteps - 1);
-}
 }  // namespace
 
 int iso2d_run(const Grid &g, const Fields &F, long nsteps, long it0, const RunExtract &ex, unsigned *sync_words,
-              const RunTiles *tiles, cudaStream_t s) {
+              cudaStream_t s) {
     if (g.ndim != 2) return -1;
-    static int cap = 0, cap_nbr = 0;
+    static int cap = 0;
     if (!cap) {
-        int dev = 0, sms = 0, per = 0, per_n = 0, coop = 0;
+        int dev = 0, sms = 0, per = 0, coop = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_iso2d_run, NT, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_n, k_iso2d_run_nbr, NT, 0);
         cap = coop && per > 0 ? sms * per : -1;
-        cap_nbr = coop && per_n > 0 ? sms * per_n : -1;
     }
     if (cap <= 0) return -1;
     const long ntiles = ((g.nz + TZ - 1) / TZ) * ((g.nx + TX - 1) / TX);
-    if (tiles && ntiles <= cap_nbr) {
-        // one CTA per tile, all co-resident
-        Grid gg = g;
-        Fields FF = F;
-        long ns = nsteps, i0 = it0;
-        RunExtract ee = ex;
-        unsigned *st = sync_words + 2, *fl = tiles->flags;
-        const int *ts = tiles->tstart, *tg = tiles->tgroups;
-        void *args[] = {&gg, &FF, &ns, &i0, &ee, &st, &fl, &ts, &tg};
-        return cudaLaunchCooperativeKernel((const void *)k_iso2d_run_nbr, dim3((unsigned)ntiles), dim3(NT), args, 0,
-                                           s) == cudaSuccess
-                   ? 0
-                   : 1;
-    }
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     Grid gg = g;
     Fields FF = F;

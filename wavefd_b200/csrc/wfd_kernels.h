@@ -50,14 +50,6 @@ struct RunExtract {
     long nt;
 };
 
-// Neighbour-synchronised whole-loop run of the 2D Iso kernel: one step counter per tile (zeroed before
-// the launch) and the receiver groups each tile extracts (tgroups[tstart[t] .. tstart[t+1])).
-struct RunTiles {
-    unsigned *flags;
-    const int *tstart, *tgroups;
-};
-constexpr int ISO2D_TILE_X = 16, ISO2D_TILE_Z = 64;  // the 2D Iso kernels' tile (x rows, z columns)
-
 struct Fields {
     float *v, *b, *q, *eps, *eta, *f, *st, *ct, *sp, *cp;
     float *pcur, *pold, *pspace, *mcur, *mold, *mspace;
@@ -121,7 +113,7 @@ struct TileInfo {
     bool fused_aniso2d(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);  \
     /* whole 2D Iso time loop in one cooperative launch: 0 launched, -1 not available, 1 launch error */ \
     int iso2d_run(const wfd::Grid &g, const wfd::Fields &F, long nsteps, long it0, const wfd::RunExtract &ex, \
-                  unsigned *sync_words, const wfd::RunTiles *tiles, cudaStream_t s);                     \
+                  unsigned *sync_words, cudaStream_t s);                                                 \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \

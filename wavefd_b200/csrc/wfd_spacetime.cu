@@ -14,7 +14,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -431,65 +430,15 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
         if (!wfd::ensure_scratch(p, p->phys == wfd::ISO ? 3 : 6)) return p->status;
     const bool run2d = p->ndim == 2 && p->phys == wfd::ISO && p->fused && !p->illum && nsteps > 0 &&
                        (!src || src->t.ngroups <= 1024);
-    // 2D Iso whole-loop run with neighbour-only synchronisation: a step counter per tile and the
-    // receiver groups split over the tiles, each group to the tile of its first cell when all its
-    // cells lie in that tile or its neighbours (else the grid-wide barrier version runs)
-    const long ntz = (p->nz + wfd::ISO2D_TILE_Z - 1) / wfd::ISO2D_TILE_Z;
-    const long ntiles = ntz * ((p->nx + wfd::ISO2D_TILE_X - 1) / wfd::ISO2D_TILE_X);
-    std::vector<int> tstart, tgroups;
-    // WAVEFD_B200_RUN2D=barrier keeps the grid-wide barrier version (for comparisons)
-    const char *run_mode = getenv("WAVEFD_B200_RUN2D");
-    bool by_tiles = run2d && ntiles < (1L << 20) && !(run_mode && strcmp(run_mode, "barrier") == 0);
-    if (by_tiles && rec && rec->t.ngroups) {
-        const auto &t = rec->t;
-        std::vector<long> owner(t.ngroups);
-        auto tile_xz = [&](long k, long &tx, long &tz) {
-            tx = (k / p->nz) / wfd::ISO2D_TILE_X;
-            tz = (k % p->nz) / wfd::ISO2D_TILE_Z;
-        };
-        for (long gi = 0; gi < t.ngroups && by_tiles; gi++) {
-            long tx0, tz0;
-            tile_xz(t.other[t.start[gi]], tx0, tz0);
-            for (long j = t.start[gi]; j < t.start[gi + 1]; j++) {
-                long tx, tz;
-                tile_xz(t.other[j], tx, tz);
-                if (labs(tx - tx0) > 1 || labs(tz - tz0) > 1) by_tiles = false;
-            }
-            owner[gi] = tx0 * ntz + tz0;
-        }
-        if (by_tiles) {
-            tstart.assign(ntiles + 1, 0);
-            for (long gi = 0; gi < t.ngroups; gi++) tstart[owner[gi] + 1]++;
-            for (long i = 0; i < ntiles; i++) tstart[i + 1] += tstart[i];
-            tgroups.resize(t.ngroups);
-            std::vector<int> fill(tstart.begin(), tstart.end() - 1);
-            for (long gi = 0; gi < t.ngroups; gi++) tgroups[fill[owner[gi]]++] = (int)gi;
-        }
-    } else if (by_tiles) {
-        tstart.assign(ntiles + 1, 0);
-    }
-    // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch;
-    // d_it[2..3]: the barrier words of the persistent 2D loop (count, generation, status); then, for
-    // the neighbour-synchronised 2D run, the tile step counters and the tiles' group lists
-    const size_t head = 4 * sizeof(long);
-    const size_t nflags = by_tiles ? (size_t)ntiles : 0;
-    const size_t bytes = head + sizeof(unsigned) * nflags + sizeof(int) * (tstart.size() + tgroups.size());
     long *d_it = nullptr;
-    if (wfd::dMallocAsync(&d_it, bytes, s) != cudaSuccess)
+    // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch;
+    // d_it[2..3]: the barrier words of the persistent 2D loop (count, generation, status)
+    if (wfd::dMallocAsync(&d_it, 4 * sizeof(long), s) != cudaSuccess)
         return wfd::prop_fail(p, WFD_ERR_ALLOC, "time index allocation failed");
-    std::vector<char> init(bytes, 0);
-    reinterpret_cast<long *>(init.data())[0] = it0;
-    unsigned *d_flags = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(d_it) + head);
-    int *d_tstart = reinterpret_cast<int *>(d_flags + nflags);
-    int *d_tgroups = d_tstart + tstart.size();
-    if (!tstart.empty()) memcpy(init.data() + head + sizeof(unsigned) * nflags, tstart.data(), sizeof(int) * tstart.size());
-    if (!tgroups.empty())
-        memcpy(init.data() + head + sizeof(unsigned) * nflags + sizeof(int) * tstart.size(), tgroups.data(),
-               sizeof(int) * tgroups.size());
-    cudaMemcpyAsync(d_it, init.data(), bytes, cudaMemcpyHostToDevice, s);
+    const long init[4] = {it0, 0, 0, 0};
+    cudaMemcpyAsync(d_it, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
-    // 2D Iso: the whole loop in one cooperative launch (neighbour-only synchronisation, or a grid-wide
-    // barrier between steps)
+    // 2D Iso: the whole loop in one cooperative launch (grid-wide barrier between steps)
     if (run2d) {
         wfd::Fields F = p->fields();
         F.inj = wfd::StepInject{};
@@ -501,17 +450,15 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
             ex = wfd::RunExtract{rec->t.ngroups, rec->t.d_key, rec->t.d_start, rec->t.d_other, rec->t.d_c, traces, nt};
         unsigned *words = reinterpret_cast<unsigned *>(d_it + 2);
         const wfd::Grid g = p->grid();
-        const wfd::RunTiles tiles{d_flags, d_tstart, d_tgroups};
-        const wfd::RunTiles *tp = by_tiles ? &tiles : nullptr;
-        const int r = p->strict ? wfd_strict::iso2d_run(g, F, nsteps, it0, ex, words, tp, s)
-                                : wfd_fast::iso2d_run(g, F, nsteps, it0, ex, words, tp, s);
+        const int r = p->strict ? wfd_strict::iso2d_run(g, F, nsteps, it0, ex, words, s)
+                                : wfd_fast::iso2d_run(g, F, nsteps, it0, ex, words, s);
         if (r == 0) {
             unsigned status = 0;
             cudaMemcpyAsync(&status, words + 2, sizeof status, cudaMemcpyDeviceToHost, s);
             const cudaError_t e = cudaStreamSynchronize(s);
             cudaFreeAsync(d_it, s);
             if (e != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, std::string("time loop: ") + cudaGetErrorString(e));
-            if (status) return wfd::prop_fail(p, WFD_ERR_TIMEOUT, "time loop: a wait between steps timed out");
+            if (status) return wfd::prop_fail(p, WFD_ERR_TIMEOUT, "time loop: a grid-wide barrier timed out");
             if (nsteps & 1) std::swap(p->field[wfd::F_PCUR], p->field[wfd::F_POLD]);
             p->steps += nsteps;
             p->step_kernels = 1;
