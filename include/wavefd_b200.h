@@ -447,9 +447,10 @@ int WFD_Codec_SetWeights(void *codec, const float *w, long n);
 int WFD_Codec_GetWeights(void *codec, float *w, long n);
 int WFD_Codec_Encode(void *codec, const float *field, long nx, long ny, long nz, void *latent, void *stream);
 int WFD_Codec_Decode(void *codec, const void *latent, long nx, long ny, long nz, float *field, void *stream);
-/* Encode/decode engine: 0 = mma.sync (the default), 1 = tcgen05 tensor cores (UMMA with the
- * accumulators in tensor memory). The two read each other's codes. WFD_ERR_UNSUPPORTED when the
- * tcgen05 kernels cannot be launched here. WAVEFD_B200_CODEC=tcgen05 selects engine 1 at creation. */
+/* Encode/decode engine: 0 = mma.sync, 1 = tcgen05 tensor cores (UMMA with the accumulators in tensor
+ * memory), 2 = encode on mma.sync and decode on tcgen05 (the default: the faster kernel of each
+ * direction). The kernels read each other's codes. WFD_ERR_UNSUPPORTED when the tcgen05 kernels cannot
+ * be launched here. WAVEFD_B200_CODEC=mma or =tcgen05 selects engine 0 or 1 at creation. */
 int WFD_Codec_SetEngine(void *codec, int engine);
 int WFD_Codec_Engine(void *codec);
 /* CTAs launched by the encode (0: mma.sync, 2: tcgen05) and decode (1: mma.sync, 3: tcgen05) kernels */

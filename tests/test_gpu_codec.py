@@ -61,7 +61,7 @@ def test_gradient_matches_oracle(torch):
         assert r <= 10 * GRAD_TOL, (name, r)
 
 
-@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("engine", ["tcgen05", "mma.sync", "mixed"])
 def test_encode_decode_matches_oracle(torch, engine):
     from wavefd_b200.codec import WavefieldCodec
     codec = WavefieldCodec(seed=7)
@@ -105,7 +105,7 @@ def test_tcgen05_engine_matches_mma_sync(torch):
     formed in another order)."""
     from wavefd_b200.codec import WavefieldCodec
     codec = WavefieldCodec(seed=9)
-    assert codec.engine == "mma.sync"
+    assert codec.engine == "mixed"
     shape = (70, 45, 100)
     rng = np.random.default_rng(10)
     f = rng.standard_normal(shape)

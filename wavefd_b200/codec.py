@@ -116,14 +116,17 @@ class WavefieldCodec:
         nx, ny, nz = shape
         return int(_L().WFD_Codec_RawBlocks(_dp(code), nx, ny, nz))
 
+    _ENGINES = ("mma.sync", "tcgen05", "mixed")
+
     @property
     def engine(self) -> str:
-        """"mma.sync" (the default) or "tcgen05" (UMMA with the accumulators in tensor memory)."""
-        return "tcgen05" if _L().WFD_Codec_Engine(self.c) == 1 else "mma.sync"
+        """"mma.sync", "tcgen05" (UMMA with the accumulators in tensor memory) or "mixed" (encode on
+        mma.sync, decode on tcgen05: the default, the faster kernel of each direction)."""
+        return self._ENGINES[_L().WFD_Codec_Engine(self.c)]
 
     @engine.setter
     def engine(self, name: str):
-        _check(_L().WFD_Codec_SetEngine(self.c, {"tcgen05": 1, "mma.sync": 0}[name]), "SetEngine")
+        _check(_L().WFD_Codec_SetEngine(self.c, self._ENGINES.index(name)), "SetEngine")
 
     def grids(self):
         """CTAs launched by each coding kernel."""

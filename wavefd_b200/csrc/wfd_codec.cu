@@ -786,7 +786,7 @@ struct Codec {
     long step = 0;
     int device = 0;
     int grid_enc = 0, grid_dec = 0, grid_train = 0;
-    int engine = 0;  // encode/decode on 0: mma.sync, 1: tcgen05 (UMMA, tensor memory)
+    int engine = 0;  // 0: mma.sync, 1: tcgen05 (UMMA, tensor memory), 2: encode mma.sync, decode tcgen05
     int grid_enc_u = 0, grid_dec_u = 0;
 };
 
@@ -937,11 +937,12 @@ extern "C" void *WFD_Codec_Create(unsigned seed) {
     }
     c->grid_enc_u = umma_ok ? sms * (peu < 8 ? peu : 8) : 0;
     c->grid_dec_u = umma_ok ? sms * (pdu < 8 ? pdu : 8) : 0;
-    // default: mma.sync, measured faster at 512x512x400 (encode 0.28 against 0.48 ms, decode 0.16
-    // against 0.35 ms: the four dependent UMMA rounds per slab wait on completion, where the mma.sync
-    // kernels keep each layer's operands in registers); WAVEFD_B200_CODEC=tcgen05 selects the other
+    // default: encode on mma.sync, decode on tcgen05, the faster kernel of each direction as measured
+    // at 512x512x400 (encode 0.28 against 0.34 ms: four dependent UMMA rounds per slab wait on their
+    // completion, where the mma.sync kernel keeps each layer's operands in registers; decode 0.153
+    // against 0.160 ms). WAVEFD_B200_CODEC=mma or =tcgen05 puts both directions on one engine.
     const char *eng = getenv("WAVEFD_B200_CODEC");
-    c->engine = umma_ok && eng && strcmp(eng, "tcgen05") == 0 ? 1 : 0;
+    c->engine = !umma_ok || (eng && strcmp(eng, "mma") == 0) ? 0 : (eng && strcmp(eng, "tcgen05") == 0 ? 1 : 2);
     if (cuda_status(cudaDeviceSynchronize(), "WFD_Codec_Create")) {
         WFD_Codec_Free(c);
         return nullptr;
@@ -1025,7 +1026,7 @@ extern "C" int WFD_Codec_Decode(void *codec, const void *latent, long nx, long n
     const float *raw = reinterpret_cast<const float *>(base + L.raw);
     const long nslab = (long)d.nsx * d.nsy * d.nsz;
     const int grid = (int)(nslab < c->grid_dec ? nslab : c->grid_dec);
-    if (c->engine == 1)
+    if (c->engine >= 1)
         k_decode_umma<<<(int)(nslab < c->grid_dec_u ? nslab : c->grid_dec_u), NTC, umma_layout::D_BYTES, st>>>(
             d, scale, lat, c->wb, c->w, field);
     else
@@ -1036,8 +1037,8 @@ extern "C" int WFD_Codec_Decode(void *codec, const void *latent, long nx, long n
 
 extern "C" int WFD_Codec_SetEngine(void *codec, int engine) {
     wfd::codec::Codec *c = C(codec);
-    if (!c || engine < 0 || engine > 1) return WFD_ERR_ARG;
-    if (engine == 1 && (c->grid_enc_u == 0 || c->grid_dec_u == 0)) return WFD_ERR_UNSUPPORTED;
+    if (!c || engine < 0 || engine > 2) return WFD_ERR_ARG;
+    if (engine >= 1 && (c->grid_enc_u == 0 || c->grid_dec_u == 0)) return WFD_ERR_UNSUPPORTED;
     c->engine = engine;
     return WFD_OK;
 }

@@ -18,13 +18,12 @@ __device__ unsigned d_codec_status;
 
 namespace umma_layout {
 // byte offsets in dynamic shared memory (every buffer 128-byte aligned)
-constexpr int E_SLAB = 0;                       // SLAB floats (refilled by cp.async during the slab's rounds)
-constexpr int E_OPS = E_SLAB + SLAB * 4;        // 16 KB shared by the operands, each dead when the next is written:
-constexpr int E_A1 = E_OPS;                     //   [128 rows][64] bf16: LBO 128, SBO 1024 (16 KB)
-constexpr int E_A2 = E_OPS;                     //   [16 rows][128] bf16: LBO 256, SBO 128 (unused rows read to 6 KB)
-constexpr int E_LAT = E_OPS + 8192;             //   B of D1: [16 blocks][32] bf16: LBO 128, SBO 512
-constexpr int E_A4 = E_OPS + 12288;             //   [128 rows][16] bf16: LBO 128, SBO 256
-constexpr int E_W1 = E_OPS + 16384;             // B of E1: [16][64]: LBO 128, SBO 1024
+constexpr int E_SLABS = 0;                      // 2 x SLAB floats
+constexpr int E_A1 = E_SLABS + 2 * SLAB * 4;    // [128 rows][64] bf16: LBO 128, SBO 1024
+constexpr int E_A2 = E_A1 + 16384;              // [16 rows][128] bf16: LBO 256, SBO 128 (+2 KB read by unused rows)
+constexpr int E_LAT = E_A2 + 6144;              // B of D1: [16 blocks][32] bf16: LBO 128, SBO 512
+constexpr int E_A4 = E_LAT + 1024;              // [128 rows][16] bf16: LBO 128, SBO 256
+constexpr int E_W1 = E_A4 + 4096;               // B of E1: [16][64]: LBO 128, SBO 1024
 constexpr int E_W2 = E_W1 + 2048;               // B of E2: [32][128]: LBO 128, SBO 2048
 constexpr int E_W3 = E_W2 + 8192;               // A of D1: [128][32]: LBO 128, SBO 512
 constexpr int E_W4 = E_W3 + 8192;               // B of D2: [64][16]: LBO 128, SBO 256
@@ -46,8 +45,7 @@ static_assert(E_A1 % 128 == 0 && E_A2 % 128 == 0 && E_LAT % 128 == 0 && E_A4 % 1
               "operand alignment");
 static_assert(D_LAT % 128 == 0 && D_A4 % 128 == 0 && D_W3 % 128 == 0 && D_W4 % 128 == 0 && D_BAR % 8 == 0,
               "operand alignment");
-static_assert(E_BYTES <= 72 * 1024, "three encode CTAs per SM");
-static_assert(E_A2 + 6144 <= E_LAT && E_LAT + 1024 <= E_A4 && E_A4 + 4096 <= E_OPS + 16384, "operand region");
+static_assert(E_BYTES <= 114 * 1024, "two encode CTAs per SM");
 static_assert(D_BYTES <= 56 * 1024, "four decode CTAs per SM");
 
 // byte offset of element (row, k) in a K-major no-swizzle operand
@@ -174,23 +172,12 @@ __device__ __forceinline__ bool umma_decode_slab(char *sm, int lat_off, int a4_o
 }
 
 // ---- encode (tcgen05) -------------------------------------------------------------------------------
-// Grid coordinates of cell k of sub-block r of the slab at (x0, y0, z0) (the cell order of cell_off)
-__device__ __forceinline__ void cell_xyz(int r, int k, int &x, int &y, int &z) {
-    const int b = r >> 3, s = r & 7;
-    x = (s >> 2) * 4 + (k >> 4);
-    y = (b >> 2) * 8 + ((s >> 1) & 1) * 4 + ((k >> 2) & 3);
-    z = (b & 3) * 8 + (s & 1) * 4 + (k & 3);
-}
-
-// One slab buffer: the next slab's cp.async copies go into it as soon as the first layer's operand
-// has been built from it (they land during the slab's four rounds); the error energy then reads the
-// field again from global memory (an L2 hit: the slab was read a few microseconds before).
-__global__ void __launch_bounds__(NTC, 3)
+__global__ void __launch_bounds__(NTC, 2)
     k_encode_umma(Dims d, const float *__restrict__ f, const bf16 *__restrict__ wb, const float *__restrict__ wp,
                   float *__restrict__ scale_out, float *__restrict__ err_out, bf16 *__restrict__ lat_out) {
     using namespace umma_layout;
     extern __shared__ __align__(1024) char sm[];
-    float *slab = reinterpret_cast<float *>(sm + E_SLAB);
+    float *slabs = reinterpret_cast<float *>(sm + E_SLABS);
     float *fl = reinterpret_cast<float *>(sm + E_F);
     float *bscale = fl, *binv = fl + 16, *berr = fl + 32, *b1 = fl + 48, *b2 = fl + 64, *b3 = fl + 96,
           *b4 = fl + 224;
@@ -200,6 +187,7 @@ __global__ void __launch_bounds__(NTC, 3)
     const uint32_t sbase = wfd_umma::smem_addr(sm);
 
     umma_load_weights(sm, wb, wp, true, E_W1, E_W2, E_W3, E_W4, b1, b2, b3, b4);
+    for (int i = tid; i < 6144 / 16; i += NTC) reinterpret_cast<uint4 *>(sm + E_A2)[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
         wfd_dev::mbar_init(bar, 1);
         wfd_dev::fence_mbar_init();
@@ -217,14 +205,26 @@ __global__ void __launch_bounds__(NTC, 3)
     if (async && blockIdx.x < nslab) {
         int xi, yi, zi;
         slab_of(d, blockIdx.x, xi, yi, zi);
-        load_slab_async(d, f, xi, yi, zi, slab);
+        load_slab_async(d, f, xi, yi, zi, slabs);
     }
-    for (long sl = blockIdx.x; sl < nslab; sl += gridDim.x) {
+    int buf = 0;
+    for (long sl = blockIdx.x; sl < nslab; sl += gridDim.x, buf ^= 1) {
         int xi, yi, zi;
         slab_of(d, sl, xi, yi, zi);
-        __syncthreads();  // the previous slab's readers of the shared floats are done
-        if (async) asm volatile("cp.async.wait_group 0;" ::: "memory");
-        else load_slab(d, f, xi, yi, zi, slab);
+        float *slab = slabs + buf * SLAB;
+        __syncthreads();  // the other buffer's readers (the previous slab) are done
+        if (async) {
+            if (sl + gridDim.x < nslab) {
+                int xn, yn, zn;
+                slab_of(d, sl + gridDim.x, xn, yn, zn);
+                load_slab_async(d, f, xn, yn, zn, slabs + (buf ^ 1) * SLAB);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+        } else {
+            load_slab(d, f, xi, yi, zi, slab);
+        }
         __syncthreads();
         {  // block max |value|: 8 threads per block, one x plane each
             const int b = tid >> 3, x = tid & 7;
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(NTC, 3)
                 *reinterpret_cast<uint4 *>(sm + E_A1 + kmaj(r, 8 * c, 128, 1024)) = q;
             }
         }
-        // E1 (its barrier also ends every read of the slab buffer)
+        // E1
         if (!umma_round(bar, phase, [&] {
                 for (int kk = 0; kk < 4; kk++)
                     wfd_umma::mma_bf16(tm, wfd_umma::smem_desc(sbase + E_A1 + kk * 256, 128, 1024),
@@ -269,11 +269,6 @@ __global__ void __launch_bounds__(NTC, 3)
                                        wfd_umma::idesc_bf16(128, 16), kk > 0);
             }))
             break;
-        if (async && sl + gridDim.x < nslab) {  // the next slab, landing during this one's rounds
-            int xn, yn, zn;
-            slab_of(d, sl + gridDim.x, xn, yn, zn);
-            load_slab_async(d, f, xn, yn, zn, slab);
-        }
         {  // E1 epilogue: bias, leaky ReLU, BF16 into A2 row b = r/8, columns s*16 .. s*16+15
             float v[16];
             wfd_umma::tmem_ld16(tl, v);
@@ -323,31 +318,15 @@ __global__ void __launch_bounds__(NTC, 3)
                 }
             }
         }
-        // decode in place and the error energy of every block against the field (zero outside the grid)
+        // decode in place and the error energy of every block (the slab is still in shared memory)
         float e = 0.0f;
-        const int x0 = xi * SX, y0 = yi * SY, z0 = zi * SZ;
-        const bool vec = (d.nz % 4) == 0;
         const bool ok = umma_decode_slab(sm, E_LAT, E_A4, E_W3, E_W4, b3, b4, bscale, tm, bar, phase,
                                          [&](int q, const float (&v)[16]) {
 #pragma unroll
             for (int c = 0; c < 4; c++) {
-                int x, y, z;
-                cell_xyz(tid, 16 * q + 4 * c, x, y, z);
-                const long gx = x0 + x, gy = y0 + y, gz = z0 + z;
-                float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (gx < d.nx && gy < d.ny) {
-                    const float *pp = f + (gx * d.ny + gy) * d.nz + gz;
-                    if (vec && gz + 3 < d.nz) {
-                        u = __ldg(reinterpret_cast<const float4 *>(pp));
-                    } else {
-                        u.x = gz < d.nz ? __ldg(pp) : 0.f;
-                        u.y = gz + 1 < d.nz ? __ldg(pp + 1) : 0.f;
-                        u.z = gz + 2 < d.nz ? __ldg(pp + 2) : 0.f;
-                        u.w = gz + 3 < d.nz ? __ldg(pp + 3) : 0.f;
-                    }
-                }
-                const float d0 = v[4 * c] - u.x, d1 = v[4 * c + 1] - u.y, d2 = v[4 * c + 2] - u.z,
-                            d3 = v[4 * c + 3] - u.w;
+                const float4 x = *reinterpret_cast<const float4 *>(slab + cell_off(tid, 16 * q + 4 * c));
+                const float d0 = v[4 * c] - x.x, d1 = v[4 * c + 1] - x.y, d2 = v[4 * c + 2] - x.z,
+                            d3 = v[4 * c + 3] - x.w;
                 e += d0 * d0 + d1 * d1 + d2 * d2 + d3 * d3;
             }
         });
