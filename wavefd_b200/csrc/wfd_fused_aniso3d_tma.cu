@@ -27,7 +27,6 @@
 // in a device status word and leaves. Requires nz % 4 == 0 (TMA row pitch).
 #include "wfd_kernels.h"
 #include "wfd_tma.cuh"
-#include "wfd_umma.cuh"
 
 namespace WFD_NS {
 using namespace wfd;
@@ -143,11 +142,9 @@ struct Out6 {
 // Pass 1 at the cell pair with extended row er (y = y0-4+er) and extended column ec (z = z0-4+ec)
 // of the lead plane. WHICH: 0 = all six outputs, 1 = y outputs only, 2 = z outputs only.
 // ring[i] = ring slot of plane P-3+i. ok = the reference computes this cell's outputs.
-// With XW (the tile pair), the x window of pCur/mCur (planes P-3 .. P+4) comes from xp/xm, which the
-// thread keeps in tensor memory, instead of eight ring loads per field.
-template <int PHYS, int WHICH, bool XW = false>
+template <int PHYS, int WHICH>
 __device__ __forceinline__ Out6 pass1(const Grid &g, const float *const (&ring)[8], const float *mat, int er, int ec,
-                                      bool ok, bool zero_xy, const float2 *xp = nullptr, const float2 *xm = nullptr) {
+                                      bool ok, bool zero_xy) {
     const int off = (er + 3) * RZW + ec + 4;
     const float *cp = ring[3] + off;  // centre plane, this pair
     const bool need_x = WHICH == 0 || PHYS == TTI;
@@ -155,10 +152,7 @@ __device__ __forceinline__ Out6 pass1(const Grid &g, const float *const (&ring)[
     const bool need_z = WHICH != 1 || PHYS == TTI;
     const float2 zero = bc2(0.0f);
     float2 dPx = zero, dPy = zero, dPz = zero, dMx = zero, dMy = zero, dMz = zero;
-    if (need_x && XW) {
-        dPx = st8d(g, g.idx, xp[0], xp[1], xp[2], xp[3], xp[4], xp[5], xp[6], xp[7]);
-        dMx = st8d(g, g.idx, xm[0], xm[1], xm[2], xm[3], xm[4], xm[5], xm[6], xm[7]);
-    } else if (need_x) {
+    if (need_x) {
         dPx = st8d(g, g.idx, ld2(ring[0] + off), ld2(ring[1] + off), ld2(ring[2] + off), ld2(ring[3] + off),
                    ld2(ring[4] + off), ld2(ring[5] + off), ld2(ring[6] + off), ld2(ring[7] + off));
         const int o = off + RBOX;
@@ -276,22 +270,6 @@ __device__ __forceinline__ void queue_phase(const Grid &g, float2 (&qx)[8][2], f
     hj[1] = qh[PH & 3][1];
 }
 
-// The tile pair's x window at phase PH = q & 7: tensor-memory slot s (columns 4s .. 4s+3: pCur
-// pair, mCur pair) holds plane jstart + s (mod 8), so planes P-3 .. P+3 of iteration q sit in slots
-// PH .. PH+6 and plane P+4, just landed in the ring, is (np, nm).
-template <int PH>
-__device__ __forceinline__ void x_window(const float (&v)[32], float2 np, float2 nm, float2 (&xp)[8],
-                                         float2 (&xm)[8]) {
-#pragma unroll
-    for (int i = 0; i < 7; i++) {
-        const int sl = (PH + i) & 7;
-        xp[i] = make_float2(v[4 * sl], v[4 * sl + 1]);
-        xm[i] = make_float2(v[4 * sl + 2], v[4 * sl + 3]);
-    }
-    xp[7] = np;
-    xm[7] = nm;
-}
-
 // BATCH = false: one propagator object, tensor maps in the kernel parameters, static items.
 // BATCH = true: many shots; each item names its shot, whose sizes, output pointers and tensor maps
 // sit in a descriptor in global memory; CTAs take items from a shared counter.
@@ -307,7 +285,6 @@ __global__ void __launch_bounds__(NT, 1)
     uint64_t *mbar = rbar + NR;
     int *abort_flag = reinterpret_cast<int *>(mbar + NM);
     int *item_slot = abort_flag + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(item_slot + 1);
     constexpr int nmat = PHYS == TTI ? 8 : 4;
 
     const int tid = threadIdx.x;
@@ -318,13 +295,7 @@ __global__ void __launch_bounds__(NT, 1)
         *abort_flag = 0;
     }
     for (int i = tid; i < 2 * TYR * TZ + 2 * TY * TZW; i += NT) TYs[i] = 0.0f;
-    // tensor memory: each thread's lane holds its tile pair's pCur/mCur of the last 8 planes (32
-    // columns; warps w and w + 4 share a lane quarter, so 64 columns)
-    if (tid < 32) wfd_umma::tmem_alloc(tmem_slot, 64);
-    wfd_umma::fence_before_sync();
     __syncthreads();
-    wfd_umma::fence_after_sync();
-    const uint32_t tq = *tmem_slot + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16) + (tid >= 128 ? 32u : 0u);
 
     // this thread's tile pair (row, zp) and halo pair
     const int zp = tid & 15;
@@ -464,15 +435,6 @@ __global__ void __launch_bounds__(NT, 1)
         }
         __syncthreads();
 
-        {  // the tile pair's x window: planes jstart .. jstart+6 into tensor-memory slots 0 .. 6
-            const int off = (row + 7) * RZW + 8 + 2 * zp;
-            const unsigned r0 = rseq % NR;
-#pragma unroll
-            for (int i = 0; i < 7; i++) {
-                const float *rp = sm + OFF_RING + ((r0 + i) % NR) * R_SLOT + off;
-                wfd_umma::tmem_st4(tq + 4 * i, rp[0], rp[1], rp[RBOX], rp[RBOX + 1]);
-            }
-        }
         float2 qx[8][2], qc[4][4], qh[4][2];
 #pragma unroll
         for (int i = 0; i < 8; i++) qx[i][0] = qx[i][1] = bc2(0.0f);
@@ -541,30 +503,8 @@ __global__ void __launch_bounds__(NT, 1)
             const float *mat = sm + OFF_MAT + (ms % NM) * M_STAGE;
             const bool pin = P >= 4 && P < g.nx - 4;
 
-            // the tile pair's x window: planes P-3 .. P+3 from tensor memory, P+4 from the ring (and into
-            // tensor memory, over plane P-4)
-            float2 xp[8], xm[8];
-            {
-                const int off = (row + 7) * RZW + 8 + 2 * zp;
-                wfd_umma::tmem_wait_st();
-                float v[32];
-                wfd_umma::tmem_ld32(tq, v);
-                const float2 np = ld2(ring[7] + off), nm = ld2(ring[7] + RBOX + off);
-                switch (q & 7) {
-                    case 0: x_window<0>(v, np, nm, xp, xm); break;
-                    case 1: x_window<1>(v, np, nm, xp, xm); break;
-                    case 2: x_window<2>(v, np, nm, xp, xm); break;
-                    case 3: x_window<3>(v, np, nm, xp, xm); break;
-                    case 4: x_window<4>(v, np, nm, xp, xm); break;
-                    case 5: x_window<5>(v, np, nm, xp, xm); break;
-                    case 6: x_window<6>(v, np, nm, xp, xm); break;
-                    default: x_window<7>(v, np, nm, xp, xm); break;
-                }
-                wfd_umma::tmem_st4(tq + 4 * ((q + 7) & 7), np.x, np.y, nm.x, nm.y);
-            }
             // pass 1 at the lead plane: the tile pair, then the halo pair
-            const Out6 c = pass1<PHYS, 0, true>(g, ring, mat, row + 4, 4 + 2 * zp, pin && yz_tile, top && zp == 0,
-                                                xp, xm);
+            const Out6 c = pass1<PHYS, 0>(g, ring, mat, row + 4, 4 + 2 * zp, pin && yz_tile, top && zp == 0);
             float2 h0 = bc2(0.0f), h1 = bc2(0.0f);
             // (the z-halo pairs above the free surface hold images, written by the tile pairs)
             if (h_kind == 1) {
@@ -631,13 +571,14 @@ __global__ void __launch_bounds__(NT, 1)
                 const float2 V = ld2(cs + C_V * CBOX + o), Q = ld2(cs + C_Q * CBOX + o), B = ld2(cs + C_B * CBOX + o);
                 const float2 k2 = div2(mul2(mul2(bc2(g.dt2), V), V), B);
                 const long k = j * g.sx + (long)y * g.nz + z;
+                const int ro = (row + 7) * RZW + 8 + 2 * zp;
                 // Born-V injection fused after the step (prop3DAcoTTIDenQ_DEO2_FDTD.h:423-452):
                 // new += 2 dt^2 dV/V * DP (DM), every cell
                 float2 bfac = bc2(0.0f);
                 if (EPI && F.epi.born_dv) bfac = div2(mul2(bc2(2.0f * g.dt * g.dt), ea), V);
 #pragma unroll
                 for (int f = 0; f < 2; f++) {
-                    const float2 pc = f == 0 ? xp[0] : xm[0];  // plane j = P-3
+                    const float2 pc = ld2(ring[0] + f * RBOX + ro);
                     const float2 po = ld2(cs + (f == 0 ? C_PO : C_MO) * CBOX + o);
                     const float2 t = sub2(sub2(mul2(k2, L[f]), mul2(Q, sub2(pc, po))), po);
                     const float2 np = add2(t, mul2(bc2(2.0f), pc));
@@ -654,14 +595,14 @@ __global__ void __launch_bounds__(NT, 1)
                 if (EPI && F.epi.img) {
                     // imaging condition fused after the step (.h:567-592): img += 2B/V^3 (DP pOld + DM
                     // mOld), pOld/mOld being this step's input pCur/mCur
-                    const float2 pcp = xp[0], pcm = xm[0];
+                    const float2 pcp = ld2(ring[0] + ro), pcm = ld2(ring[0] + RBOX + ro);
                     const float2 fac = div2(mul2(bc2(2.0f), B), mul2(mul2(V, V), V));
                     st2(F.epi.img + k, add2(ea, mul2(fac, add2(mul2(eb, pcp), mul2(ec, pcm)))));
                 }
                 if (!BATCH && F.illum) {
                     // source illumination, every cell: sum += pCur^2 (separate IEEE multiply and add,
                     // as illumination.c:31-53 does)
-                    const float2 pcp = xp[0];
+                    const float2 pcp = ld2(ring[0] + ro);
                     float2 a = ld2(F.illum + k);
                     a.x = __fadd_rn(a.x, __fmul_rn(pcp.x, pcp.x));
                     a.y = __fadd_rn(a.y, __fmul_rn(pcp.y, pcp.y));
@@ -681,13 +622,6 @@ __global__ void __launch_bounds__(NT, 1)
     if (*abort_flag && tid == ISSUER) {
         for (unsigned gi = r_done; gi < r_issued; gi++) mbar_wait(&rbar[gi % NR], (gi / NR) & 1u, 100000000ull);
         for (unsigned gi = m_done; gi < m_issued; gi++) mbar_wait(&mbar[gi % NM], (gi / NM) & 1u, 100000000ull);
-    }
-    wfd_umma::tmem_wait_st();
-    wfd_umma::fence_before_sync();
-    __syncthreads();
-    if (tid < 32) {
-        wfd_umma::fence_after_sync();
-        wfd_umma::tmem_dealloc(*tmem_slot, 64);
     }
 }
 
