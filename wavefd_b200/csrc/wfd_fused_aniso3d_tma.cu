@@ -319,15 +319,6 @@ __global__ void __launch_bounds__(NT, 1)
     }
 
     const long total = (long)ntz0 * nty0 * nch0;
-    // nch0 == 0 (single objects): this CTA's share of the (tile, plane) sequence, tile by tile, x
-    // within a tile: one contiguous span, so a tile's planes held by one CTA are swept in one pass
-    // (one warm-up) and every CTA gets the same number of planes
-    long span = 0, span_end = 0;
-    if (!BATCH && nch0 == 0) {
-        const long W = (long)ntz0 * nty0 * g0.nx;
-        span = W * blockIdx.x / gridDim.x;
-        span_end = W * (blockIdx.x + 1) / gridDim.x;
-    }
     unsigned rseq = 0, mseq = 0;      // ring planes and stages of the items finished by this CTA
     unsigned r_issued = 0, m_issued = 0;  // issued by thread 0
     unsigned r_done = 0, m_done = 0;      // landed (waits that succeeded)
@@ -361,29 +352,18 @@ __global__ void __launch_bounds__(NT, 1)
             nty = d->nty;
             xchunk = d->xchunk;
             w = it.y;
-        } else if (nch0 == 0) {
-            if (span >= span_end) break;
         } else if (wstat >= total) {
             break;
-        }
-        long xbeg, xend;
-        if (!BATCH && nch0 == 0) {
-            w = span / g.nx;
-            xbeg = span % g.nx;
-            xend = xbeg + (span_end - span) < g.nx ? xbeg + (span_end - span) : g.nx;
-            span += xend - xbeg;
         }
         const CUtensorMap *mP = maps + 0, *mM = maps + 1, *mB = maps + 2, *mE = maps + 3, *mA = maps + 4,
                           *mF = maps + 5, *mST = maps + 6, *mCT = maps + 7, *mSP = maps + 8, *mCP = maps + 9,
                           *mPO = maps + 10, *mMO = maps + 11, *mV = maps + 12, *mQ = maps + 13, *mBC = maps + 14;
         const int tzi = (int)(w % ntz);
         const int tyi = (int)((w / ntz) % nty);
+        const int chi = (int)(w / ((long)ntz * nty));
         const int z0 = tzi * TZ, y0 = tyi * TY;
-        if (BATCH || nch0 != 0) {
-            const int chi = (int)(w / ((long)ntz * nty));
-            xbeg = (long)chi * xchunk;
-            xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
-        }
+        const long xbeg = (long)chi * xchunk;
+        const long xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
         const long jstart = xbeg - WARMUP;
         const int niter = (int)(xend - jstart);
         const int nplanes = niter + 7;  // ring planes jstart .. xend+6
@@ -682,12 +662,22 @@ bool launch(const Grid &g, const Fields &F, cudaStream_t s) {
     const int ntz = (int)((g.nz + TZ - 1) / TZ);
     const int nty = (int)((g.ny + TY - 1) / TY);
     const long tiles = (long)ntz * nty;
-    // every CTA sweeps an equal contiguous span of the (tile, plane) sequence (nch = 0); CTAs with
-    // spans of fewer than 32 planes would spend most of their time on the warm-up planes
-    const long planes = tiles * g.nx;
-    const long by_span = (planes + 31) / 32;
-    const int grid = (int)(by_span < grid_cap ? by_span : grid_cap);
-    const int nch = 0, xchunk = 0;
+    int best_nch = 1;
+    double best_cost = 1e30;
+    for (int nch = 1; nch <= 64 && nch <= g.nx / 16 + 1; nch++) {
+        const long chunk = (g.nx + nch - 1) / nch;
+        const long items = tiles * nch;
+        const double waves = (double)((items + grid_cap - 1) / grid_cap);
+        const double cost = waves * (double)(chunk + WARMUP * 0.6);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best_nch = nch;
+        }
+    }
+    const int xchunk = (int)((g.nx + best_nch - 1) / best_nch);
+    const int nch = (int)((g.nx + xchunk - 1) / xchunk);
+    const long work = tiles * nch;
+    const int grid = (int)(work < grid_cap ? work : grid_cap);
     if (F.epi.born_dv || F.epi.img || F.epi.scale_space)
         k_aniso3d_tma<PHYS, LINEAR, false, true><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr,
                                                                               nullptr, nullptr, 0, nullptr);

@@ -372,15 +372,6 @@ __global__ void __launch_bounds__(NT, 3)
     __syncthreads();
 
     const long total = (long)ntz0 * nty0 * nch0;
-    // nch0 == 0 (single objects): this CTA's share of the (tile, plane) sequence, tile by tile, x
-    // within a tile: one contiguous span, so a tile's planes held by one CTA are swept in one pass
-    // (one warm-up) and every CTA gets the same number of planes
-    long span = 0, span_end = 0;
-    if (!BATCH && nch0 == 0) {
-        const long W = (long)ntz0 * nty0 * g0.nx;
-        span = W * blockIdx.x / gridDim.x;
-        span_end = W * (blockIdx.x + 1) / gridDim.x;
-    }
     unsigned gseq = 0;                  // groups consumed so far by this CTA
     unsigned out_from = 0, out_to = 0;  // groups issued but not yet consumed (thread 0)
     const int zq = lane & 7;
@@ -413,32 +404,21 @@ __global__ void __launch_bounds__(NT, 3)
             nty = d->nty;
             xchunk = d->xchunk;
             w = it.y;
-        } else if (nch0 == 0) {
-            if (span >= span_end) break;
         } else if (wstat >= total) {
             break;
         }
         const CUtensorMap *mPH = maps + 0, *mPN = maps + 1, *mBH = maps + 2, *mBN = maps + 3, *mPO = maps + 4,
                           *mV = maps + 5, *mQ = maps + 6;
-        long xbeg, xend;
-        if (!BATCH && nch0 == 0) {
-            w = span / g.nx;
-            xbeg = span % g.nx;
-            xend = xbeg + (span_end - span) < g.nx ? xbeg + (span_end - span) : g.nx;
-            span += xend - xbeg;
-        }
         const int tzi = (int)(w % ntz);
         const int tyi = (int)((w / ntz) % nty);
+        const int chi = (int)(w / ((long)ntz * nty));
         const int z0 = tzi * TZ;
         const int y0 = tyi * TY;
         const int z = z0 + 4 * zq;
         const int y = y0 + row;
         const bool own = z < g.nz && y < g.ny;
-        if (BATCH || nch0 != 0) {
-            const int chi = (int)(w / ((long)ntz * nty));
-            xbeg = (long)chi * xchunk;
-            xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
-        }
+        const long xbeg = (long)chi * xchunk;
+        const long xend = xbeg + xchunk < g.nx ? xbeg + xchunk : g.nx;
         const long jstart = xbeg - WARMUP;
         const int ngroups = (int)(xend - jstart);
         const bool tile_top = z0 == 0 && g.fs;
@@ -587,13 +567,24 @@ bool fused_iso3d_tma(const Grid &g, const Fields &F, cudaStream_t s) {
     const int grid_cap = iso_grid_cap();
     const int ntz = (int)((g.nz + TZ - 1) / TZ);
     const int nty = (int)((g.ny + TY - 1) / TY);
-    // every CTA sweeps an equal contiguous span of the (tile, plane) sequence (nch = 0); CTAs with
-    // spans of fewer than 64 planes would spend most of their time on the warm-up planes
+    // x-chunking: balance the last wave of persistent CTAs against the warm-up planes per chunk
     const long tiles = (long)ntz * nty;
-    const long planes = tiles * g.nx;
-    const long by_span = (planes + 63) / 64;
-    const int grid = (int)(by_span < grid_cap ? by_span : grid_cap);
-    const int nch = 0, xchunk = 0;
+    int best_nch = 1;
+    double best_cost = 1e30;
+    for (int nch = 1; nch <= 64 && nch <= g.nx / 16 + 1; nch++) {
+        const long chunk = (g.nx + nch - 1) / nch;
+        const long items = tiles * nch;
+        const double waves = (double)((items + grid_cap - 1) / grid_cap);
+        const double cost = waves * (double)(chunk + WARMUP * 0.35);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best_nch = nch;
+        }
+    }
+    const int xchunk = (int)((g.nx + best_nch - 1) / best_nch);
+    const int nch = (int)((g.nx + xchunk - 1) / xchunk);
+    const long work = tiles * nch;
+    const int grid = (int)(work < grid_cap ? work : grid_cap);
 if (F.epi.born_dv || F.epi.img || F.epi.scale_space)
             k_iso3d_tma<false, true><<<grid, NT, SMEM_BYTES, s>>>(g, F, M, ntz, nty, nch, xchunk, nullptr, nullptr, nullptr, 0,
                                                     nullptr);
