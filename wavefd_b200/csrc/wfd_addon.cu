@@ -94,6 +94,7 @@ extern "C" int WFD_Prop_Synchronize(void *p) { return p ? wfd::prop_sync(P(p)) :
 extern "C" int WFD_Prop_Prefetch(void *p) {
     if (!p) return WFD_ERR_ARG;
     Prop *q = P(p);
+    q->host_touched = 0;
     const size_t bytes = sizeof(float) * (size_t)q->ncells();
     for (int f = 0; f < wfd::F_COUNT; f++) {
         if (!q->field[f]) continue;

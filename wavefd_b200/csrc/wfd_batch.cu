@@ -436,8 +436,7 @@ int batch_sync(Batch *b) {
 int batch_run(Batch *b, long nsteps, long it0, bool graph) {
     if (b->status) return b->status;
     order_after_props(b);
-    if (take_host_touched())
-        for (Prop *p : b->props) prefetch_to_device(p, b->stream);
+    for (Prop *p : b->props) prefetch_touched(p, b->stream);
     if (int rc = sync_tables(b)) return rc;
     if (int rc = bcheck(b, cudaMemcpyAsync(b->d_it, &it0, sizeof(long), cudaMemcpyHostToDevice, b->stream),
                         "time index"))
@@ -512,8 +511,7 @@ float time_launches(Batch *b, int gi, int reps) {
 int batch_tune(Batch *b, int reps) {
     if (b->status) return b->status;
     order_after_props(b);
-    if (take_host_touched())
-        for (Prop *p : b->props) prefetch_to_device(p, b->stream);
+    for (Prop *p : b->props) prefetch_touched(p, b->stream);
     if (int rc = sync_tables(b)) return rc;
     const int n = (int)b->props.size();
     // save what the trial launches overwrite

@@ -17,18 +17,14 @@ namespace {
 
 Prop *P(void *p) { return reinterpret_cast<Prop *>(p); }
 
-// Host code may have written managed arrays since the last device call; move them back
-// before the kernels run (the kernels would also fault them in on demand).
-thread_local bool t_host_touched = false;
-
-void before_device(Prop *p) {
-    if (!t_host_touched) return;
-    t_host_touched = false;
-    wfd::prefetch_to_device(p, p->stream);
-}
+// Host code may have written the managed arrays it reached through getters since the object's last
+// device call; move those back before the kernels run (the kernels would also fault them in on
+// demand). Only the arrays whose getters were called: a time loop that asks for pCur every step
+// moves one array's pages, not the object's dozen.
+void before_device(Prop *p) { wfd::prefetch_touched(p, p->stream); }
 
 float *getter(void *p, int f) {
-    t_host_touched = true;
+    P(p)->host_touched |= 1u << f;
     return P(p)->field[f];
 }
 
@@ -36,10 +32,13 @@ float *getter(void *p, int f) {
 
 namespace wfd {
 
-void prefetch_to_device(Prop *p, cudaStream_t s) {
+void prefetch_touched(Prop *p, cudaStream_t s) {
+    const unsigned mask = p->host_touched;
+    if (!mask) return;
+    p->host_touched = 0;
     const size_t bytes = sizeof(float) * (size_t)p->ncells();
     for (int f = 0; f < F_COUNT; f++) {
-        if (!p->field[f]) continue;
+        if (!(mask >> f & 1u) || !p->field[f]) continue;
 #if CUDART_VERSION >= 13000
         cudaMemLocation loc{cudaMemLocationTypeDevice, p->device};
         cudaMemPrefetchAsync(p->field[f], bytes, loc, 0, s);
@@ -47,12 +46,6 @@ void prefetch_to_device(Prop *p, cudaStream_t s) {
         cudaMemPrefetchAsync(p->field[f], bytes, p->device, s);
 #endif
     }
-}
-
-bool take_host_touched() {
-    const bool t = t_host_touched;
-    t_host_touched = false;
-    return t;
 }
 
 }  // namespace wfd

@@ -39,6 +39,7 @@ struct Prop {
     int status = WFD_OK;
     std::string message;
     long steps = 0;
+    unsigned host_touched = 0;  // bit f: the getter of field f was called since the last device call
     int step_kernels = 0;  // kernels launched by the last time step (1 fused, 2 unfused)
     long run_launches = 0; // kernels launched by the last WFD_Prop_Run
     StepInject inj{};      // a source injection for the step kernel to apply (WFD_Prop_Run), or none
@@ -74,11 +75,9 @@ int global_error(std::string *msg);
 void apply_dplus2d(bool fs, long nx, long nz, float c1, float c2, float c3, float c4, float invDx, float invDz,
                    const float *inX, const float *inZ, float *outX, float *outZ);
 
-// move every array of the object to its device (managed memory written by host code through the
-// getters); take_host_touched() reports, and clears, whether a getter was called since the last
-// device call on this thread
-void prefetch_to_device(Prop *p, cudaStream_t s);
-bool take_host_touched();
+// move the arrays of the object whose getters were called since its last device call (managed
+// memory that host code may have written) back to its device, and clear that record
+void prefetch_touched(Prop *p, cudaStream_t s);
 
 // sum[i] += field[i]^2 on the device (wfd_illum.cu)
 void illum_accumulate(float *sum, const float *field, long n, cudaStream_t s);
