@@ -241,3 +241,30 @@ def test_wavefieldsep_close(lib, oracle, name, isfwi, nz):
     err = rel_l2(img - _rand(shp, 43), mine - _rand(shp, 43))
     assert err <= 1e-5, f"rel L2 of the accumulated term {err:.3e}"
     gpu.close()
+
+
+@pytest.mark.parametrize("name", ["Prop3DAcoIsoDenQ_DEO2_FDTD", "Prop3DAcoTTIDenQ_DEO2_FDTD"])
+def test_host_writes_through_getters_in_a_loop(lib, oracle, name):
+    """A time loop that asks for pCur before every step (as the reference's Julia loop does) stops
+    moving that array back to the device after two steps; host writes into it, and into the model,
+    made between steps through the getters' pointers must still reach the next step: bitwise against
+    the restatement doing the same writes."""
+    gpu, orc = _pair(lib, oracle, name, True)
+    rng = np.random.default_rng(21)
+    for it in range(8):
+        gpu.arr("PCur")  # the getter, every step
+        if it in (4, 6):  # host writes into the streaked array and into a model array
+            d = (rng.standard_normal(gpu.arr("PCur").shape) * 1e-3).astype(np.float32)
+            for r in (gpu, orc):
+                a = r.arr("PCur")
+                a[...] = a + d
+            v = gpu.arr("V")
+            v[2:5, 3:6] *= np.float32(1.01)
+            w = orc.arr("V")
+            w[2:5, 3:6] *= np.float32(1.01)
+        gpu.abi.TimeStep(gpu.p)
+        orc.step()
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(gpu.p)) == 0
+    for k in _fields(name):
+        assert same(gpu.arr(k), orc.arr(k)), f"{name} {k}: {mismatch_report(gpu.arr(k), orc.arr(k))}"
+    gpu.close()

@@ -19,8 +19,10 @@ Prop *P(void *p) { return reinterpret_cast<Prop *>(p); }
 
 // Host code may have written the managed arrays it reached through getters since the object's last
 // device call; move those back before the kernels run (the kernels would also fault them in on
-// demand). Only the arrays whose getters were called: a time loop that asks for pCur every step
-// moves one array's pages, not the object's dozen.
+// demand). Only the arrays whose getters were called, and not an array whose getter has come before
+// every one of the last two device calls: that is a time loop passing the pointer on (the reference's
+// loop asks for pCur each step), where a prefetch walks the whole array for nothing (0.43 ms for a
+// 537 MB array on a B200). Pages that host code does write in such a loop still move back, on demand.
 void before_device(Prop *p) { wfd::prefetch_touched(p, p->stream); }
 
 float *getter(void *p, int f) {
@@ -34,11 +36,16 @@ namespace wfd {
 
 void prefetch_touched(Prop *p, cudaStream_t s) {
     const unsigned mask = p->host_touched;
-    if (!mask) return;
     p->host_touched = 0;
     const size_t bytes = sizeof(float) * (size_t)p->ncells();
     for (int f = 0; f < F_COUNT; f++) {
-        if (!(mask >> f & 1u) || !p->field[f]) continue;
+        if (!(mask >> f & 1u)) {
+            p->touch_streak[f] = 0;
+            continue;
+        }
+        const bool again = p->touch_streak[f] >= 2;
+        if (p->touch_streak[f] < 255) p->touch_streak[f]++;
+        if (again || !p->field[f]) continue;
 #if CUDART_VERSION >= 13000
         cudaMemLocation loc{cudaMemLocationTypeDevice, p->device};
         cudaMemPrefetchAsync(p->field[f], bytes, loc, 0, s);

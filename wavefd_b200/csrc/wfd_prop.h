@@ -40,6 +40,7 @@ struct Prop {
     std::string message;
     long steps = 0;
     unsigned host_touched = 0;  // bit f: the getter of field f was called since the last device call
+    unsigned char touch_streak[F_COUNT] = {};  // device calls in a row preceded by that getter
     int step_kernels = 0;  // kernels launched by the last time step (1 fused, 2 unfused)
     long run_launches = 0; // kernels launched by the last WFD_Prop_Run
     StepInject inj{};      // a source injection for the step kernel to apply (WFD_Prop_Run), or none
