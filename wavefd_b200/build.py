@@ -29,6 +29,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
           "--expt-relaxed-constexpr"]
 STRICT = ["-DWFD_STRICT=1", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 FAST = ["-DWFD_STRICT=0", "-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+HOST = ["-Xcompiler", "-fopenmp"]  # host loops of the drop-in calls use the caller's thread count
 
 KERNEL_SOURCES = ["wfd_generic.cu", "wfd_fused.cu", "wfd_fused_iso3d.cu", "wfd_fused_iso3d_tma.cu",
                   "wfd_fused_aniso3d_tma.cu", "wfd_fused_vti3d_tma.cu", "wfd_fused_iso2d.cu", "wfd_fused_aniso2d.cu",
@@ -76,11 +77,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         jobs.append((os.path.join(CSRC, f), os.path.join(BUILD, stem + "_fast.o"), FAST))
     for f in HOST_SOURCES:
         stem = os.path.splitext(f)[0]
-        jobs.append((os.path.join(CSRC, f), os.path.join(BUILD, stem + ".o"), []))
+        jobs.append((os.path.join(CSRC, f), os.path.join(BUILD, stem + ".o"), HOST))
     with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         objs = list(ex.map(_compile, jobs))
     tmp = out + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "shared", "-o", tmp] + objs
+    cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "shared", "-Xcompiler", "-fopenmp", "-o", tmp] + objs
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -161,18 +161,26 @@ struct CachedTable {
     T *h_dst = nullptr, *h_src = nullptr;  // pinned host staging
 };
 
+// Host loops over the points of a drop-in call use up to the caller's thread count (the reference's
+// nthreads argument) once they are long enough to pay for it.
+constexpr long kParallelPoints = 8192;
+
 template <class T>
 bool same_points(const CachedTable<T> &e, int by_receiver, void **partitions, size_t npartitions,
-                 const long *npoints) {
+                 const long *npoints, int nth) {
     if (e.by_receiver != by_receiver || e.counts.size() != npartitions) return false;
     size_t j = 0;
     for (size_t i = 0; i < npartitions; i++) {
         if (e.counts[i] != npoints[i]) return false;
         const PointsT<T> *p = reinterpret_cast<const PointsT<T> *>(partitions[i]);
-        for (long k = 0; k < npoints[i]; k++, j++) {
-            const PointsT<T> &q = e.raw[j];
-            if (p[k].iu != q.iu || p[k].ir != q.ir || memcmp(&p[k].c, &q.c, sizeof(T)) != 0) return false;
-        }
+        const PointsT<T> *q = e.raw.data() + j;
+        const long n = npoints[i];
+        int diff = 0;
+#pragma omp parallel for num_threads(nth) if (n >= kParallelPoints) reduction(| : diff) schedule(static)
+        for (long k = 0; k < n; k++)
+            diff |= (p[k].iu != q[k].iu || p[k].ir != q[k].ir || memcmp(&p[k].c, &q[k].c, sizeof(T)) != 0) ? 1 : 0;
+        if (diff) return false;
+        j += (size_t)n;
     }
     return true;
 }
@@ -204,9 +212,9 @@ TableCache<T> &table_cache() {
 // the entry for these partitions (built and uploaded on a miss), or nullptr on allocation failure
 template <class T>
 CachedTable<T> *lookup(TableCache<T> &cache, int by_receiver, void **partitions, size_t npartitions,
-                       const long *npoints, cudaStream_t s) {
+                       const long *npoints, cudaStream_t s, int nth) {
     for (CachedTable<T> *e : cache.entries)
-        if (same_points(*e, by_receiver, partitions, npartitions, npoints)) {
+        if (same_points(*e, by_receiver, partitions, npartitions, npoints, nth)) {
             e->last_use = ++cache.clock;
             return e;
         }
@@ -244,14 +252,15 @@ CachedTable<T> *lookup(TableCache<T> &cache, int by_receiver, void **partitions,
 // read, and the current values of the locations they write, up; the new values back).
 template <class T>
 void dropin(int by_receiver, T *dst, long dst_stride, long dst_off, const T *src, long src_stride, long src_off,
-            void **partitions, size_t npartitions, const long *npoints) {
+            void **partitions, size_t npartitions, const long *npoints, size_t nthreads) {
     long total = 0;
     for (size_t i = 0; i < npartitions; i++) total += npoints[i];
     if (total <= 0) return;
+    const int nth = nthreads > 1 ? (int)(nthreads < 256 ? nthreads : 256) : 1;
     cudaStream_t s = st_stream();
     TableCache<T> &cache = table_cache<T>();
     std::lock_guard<std::mutex> lk(cache.mu);
-    CachedTable<T> *e = lookup(cache, by_receiver, partitions, npartitions, npoints, s);
+    CachedTable<T> *e = lookup(cache, by_receiver, partitions, npartitions, npoints, s, nth);
     if (!e) {
         set_global_error(WFD_ERR_ALLOC, "point table allocation failed");
         return;
@@ -261,10 +270,12 @@ void dropin(int by_receiver, T *dst, long dst_stride, long dst_off, const T *src
     const bool src_dev = device_accessible(src);
     const long ng = t.ngroups, np = t.npoints;
     if (!src_dev) {
+#pragma omp parallel for num_threads(nth) if (np >= kParallelPoints) schedule(static)
         for (long j = 0; j < np; j++) e->h_src[j] = src[t.other[j] * src_stride + src_off];
         cudaMemcpyAsync(e->d_src, e->h_src, sizeof(T) * (size_t)np, cudaMemcpyHostToDevice, s);
     }
     if (!dst_dev) {
+#pragma omp parallel for num_threads(nth) if (ng >= kParallelPoints) schedule(static)
         for (long g = 0; g < ng; g++) e->h_dst[g] = dst[t.key[g] * dst_stride + dst_off];
         cudaMemcpyAsync(e->d_dst, e->h_dst, sizeof(T) * (size_t)ng, cudaMemcpyHostToDevice, s);
     }
@@ -279,8 +290,10 @@ void dropin(int by_receiver, T *dst, long dst_stride, long dst_off, const T *src
         set_global_error(WFD_ERR_CUDA, cudaGetErrorString(err));
         return;
     }
-    if (!dst_dev)
+    if (!dst_dev) {
+#pragma omp parallel for num_threads(nth) if (ng >= kParallelPoints) schedule(static)
         for (long g = 0; g < ng; g++) dst[t.key[g] * dst_stride + dst_off] = e->h_dst[g];
+    }
 }
 
 struct DeviceTable {
@@ -295,30 +308,26 @@ using wfd::DeviceTable;
 // ---- drop-in libspacetime exports (spacetime.cc:144-204) ---------------------------------------------
 extern "C" void injectdata_float(float *field, float *data, size_t it, size_t nt, SourcePoint32 **partitions,
                                  size_t npartitions, long *npoints_per_partition, size_t nthreads) {
-    (void)nthreads;
     wfd::dropin<float>(0, field, 1, 0, data, (long)nt, (long)it - 1, (void **)partitions, npartitions,
-                       npoints_per_partition);
+                       npoints_per_partition, nthreads);
 }
 
 extern "C" void injectdata_double(double *field, double *data, size_t it, size_t nt, SourcePoint64 **partitions,
                                   size_t npartitions, long *npoints_per_partition, size_t nthreads) {
-    (void)nthreads;
     wfd::dropin<double>(0, field, 1, 0, data, (long)nt, (long)it - 1, (void **)partitions, npartitions,
-                        npoints_per_partition);
+                        npoints_per_partition, nthreads);
 }
 
 extern "C" void extractdata_float(float *data, float *field, SourcePoint32 **partitions, size_t npartitions,
                                   long *npoints_per_partition, size_t it, size_t nt, size_t nthreads) {
-    (void)nthreads;
     wfd::dropin<float>(1, data, (long)nt, (long)it - 1, field, 1, 0, (void **)partitions, npartitions,
-                       npoints_per_partition);
+                       npoints_per_partition, nthreads);
 }
 
 extern "C" void extractdata_double(double *data, double *field, SourcePoint64 **partitions, size_t npartitions,
                                    long *npoints_per_partition, size_t it, size_t nt, size_t nthreads) {
-    (void)nthreads;
     wfd::dropin<double>(1, data, (long)nt, (long)it - 1, field, 1, 0, (void **)partitions, npartitions,
-                        npoints_per_partition);
+                        npoints_per_partition, nthreads);
 }
 
 // ---- add-on: device-resident point tables ------------------------------------------------------------
