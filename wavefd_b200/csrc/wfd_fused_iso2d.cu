@@ -209,25 +209,26 @@ __global__ void __launch_bounds__(NT) k_iso2d_fused(Grid g, Fields F) {
     tile_step(g, F, (long)blockIdx.y * TX, (long)blockIdx.x * TZ, it, sm);
 }
 
-// Grid-wide barrier of the persistent run (all CTAs co-resident: cooperative launch). Sense by
-// generation: the last CTA to arrive resets the count and publishes the next generation. Every wait
-// is bounded (2 s): a CTA that gives up, or sees that another gave up, sets the status word and
-// returns false, and so does every CTA after it, so the kernel always ends.
+// Grid-wide barrier of the persistent run (all CTAs co-resident: cooperative launch). One counter
+// that only grows: barrier number gen + 1 is passed once it reaches (gen + 1) x the CTA count. Each
+// CTA adds its arrival with release semantics and polls the counter with acquire loads (no reset and
+// no separate publication: one hop fewer than a sense-reversing barrier). Every wait is bounded
+// (2 s): a CTA that gives up, or sees that another gave up, sets the status word and returns false,
+// and so does every CTA after it, so the kernel always ends.
 __device__ __forceinline__ bool grid_barrier(unsigned *words, unsigned &gen, int *ok_flag) {
-    unsigned *count = words, *pub = words + 1, *status = words + 2;
+    unsigned *count = words, *status = words + 2;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned target = gen + 1;
-        __threadfence();
-        if (atomicAdd(count, 1u) + 1 == gridDim.x) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicExch(pub, target);
-        } else {
-            uint64_t t0;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-            while (*(volatile unsigned *)pub != target) {
+        const unsigned target = (gen + 1) * gridDim.x;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        uint64_t t0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        for (unsigned spin = 1;; spin++) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if ((int)(v - target) >= 0) break;  // wrap-safe
+            if ((spin & 63) == 0) {
                 if (*(volatile unsigned *)status) {
                     ok = 0;
                     break;
@@ -239,11 +240,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned *words, unsigned &gen, int
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
             }
         }
-        __threadfence();
-        gen = target;
+        gen++;
         *ok_flag = ok;
     }
     __syncthreads();
@@ -278,7 +277,7 @@ __global__ void __launch_bounds__(NT) k_iso2d_run(Grid g, Fields F, long nsteps,
                 float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
                 float acc = *dst;
                 for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
-                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], Fs.pold[ex.other[j]]));
+                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(Fs.pold + ex.other[j])));
                 *dst = acc;
             }
         }
