@@ -47,11 +47,13 @@ def _partitions(key, iu, ir, c, nparts):
     return pp, npp, len(parts), keep
 
 
-@pytest.mark.parametrize("nparts", [1, 4])
-def test_dropin_inject_extract_host_arrays(lib, oracle, nparts):
+@pytest.mark.parametrize("nparts,npts,nr", [(1, 3000, 9), (4, 3000, 9), (3, 30000, 20000)])
+def test_dropin_inject_extract_host_arrays(lib, oracle, nparts, npts, nr):
+    """30000 points: the host loops over the points (comparison with the cached table, gather and
+    scatter of the host arrays) run on the caller's threads."""
     st = SpacetimeABI(lib)
-    ngrid, nr, nt = 4000, 9, 17
-    iu, ir, c = _points(3000, ngrid, nr, 7)
+    ngrid, nt = 40000, 17
+    iu, ir, c = _points(npts, ngrid, nr, 7)
     pp, npp, npart, keep = _partitions(iu, iu, ir, c, nparts)
     rng = np.random.default_rng(8)
     data = rng.standard_normal(nr * nt).astype(np.float32)
@@ -60,11 +62,22 @@ def test_dropin_inject_extract_host_arrays(lib, oracle, nparts):
     st.injectdata_float(fptr(f_gpu), fptr(data), 4, nt, pp, npart, npp, 4)
     oracle.inject(f_or, data, 4, nt, iu, ir, c)
     assert same(f_gpu, f_or), mismatch_report(f_gpu, f_or)
-    iu2, ir2, c2 = _points(3000, ngrid, nr, 9, sort_by="ir")
+    iu2, ir2, c2 = _points(npts, ngrid, nr, 9, sort_by="ir")
     pp2, npp2, npart2, keep2 = _partitions(ir2, iu2, ir2, c2, nparts)
     d_gpu, d_or = data.copy(), data.copy()
     st.extractdata_float(fptr(d_gpu), fptr(field), pp2, npart2, npp2, 11, nt, 4)
     oracle.extract(d_or, field, 11, nt, iu2, ir2, c2)
+    assert same(d_gpu, d_or), mismatch_report(d_gpu, d_or)
+    # the same partitions again (the cached table), then changed contents behind the same pointers
+    st.extractdata_float(fptr(d_gpu), fptr(field), pp2, npart2, npp2, 12, nt, 4)
+    oracle.extract(d_or, field, 12, nt, iu2, ir2, c2)
+    assert same(d_gpu, d_or), mismatch_report(d_gpu, d_or)
+    first = keep2[-1]
+    first[len(first) - 1].c = first[len(first) - 1].c * 0.5
+    c2 = c2.copy()
+    c2[-1] = np.float32(c2[-1] * np.float32(0.5))
+    st.extractdata_float(fptr(d_gpu), fptr(field), pp2, npart2, npp2, 13, nt, 4)
+    oracle.extract(d_or, field, 13, nt, iu2, ir2, c2)
     assert same(d_gpu, d_or), mismatch_report(d_gpu, d_or)
 
 
