@@ -356,13 +356,17 @@ def test_illumination_fused_into_step(lib, name, shape):
 
 
 @pytest.mark.parametrize("spread", ["local", "far"])
-def test_prop_run_2d_tiles(lib, spread):
+@pytest.mark.parametrize("shape", [(200, 1, 90), (1000, 1, 400)])
+def test_prop_run_2d_tiles(lib, spread, shape):
     """The 2D Iso whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each),
-    receiver groups of two points one row apart or 40 rows apart (more than two tiles), against
-    TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build)."""
+    receiver groups of two points one row apart or 40 rows apart (more than two tiles), sources in one
+    tile, on a tile corner, on the free-surface rows and outside the interior (cells the step does
+    not write), against TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build). At
+    200 x 90 (24 tiles) every tile stays in one CTA for the whole loop; at 1000 x 400 (400 tiles,
+    more than the CTAs that fit at once) the CTAs take turns over the tiles."""
     import torch
     from tests.harness import ABIRunner, make_model
-    name, shape = "Prop2DAcoIsoDenQ_DEO2_FDTD", (200, 1, 90)  # nz 200 (4 tiles), nx 90 (6 tiles)
+    name = "Prop2DAcoIsoDenQ_DEO2_FDTD"
     nz, ny, nx = shape
     nt, nsteps = 40, 17
     gap = nz * (1 if spread == "local" else 40)  # the second point of a group: 1 or 40 rows further in x
@@ -376,11 +380,18 @@ def test_prop_run_2d_tiles(lib, spread):
         g = ABIRunner(lib, name, shape, fs=True)
         lib.WFD_Prop_SetStrict(ctypes.c_void_p(g.p), 1)
         g.load(make_model(2, "iso", shape, seed=8))
-        src = (SourcePoint32 * 1)(SourcePoint32((nx // 2) * nz + 3, 1, 1.0))
-        ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), 1, 0)
+        h = nx // 2
+        spts = [SourcePoint32(h * nz + 3, 1, 1.0),             # free-surface row kz 2
+                SourcePoint32(h * nz + 6, 2, 0.5),             # the same tile
+                SourcePoint32(h * nz + 6, 1, 0.25),            # the same cell, a second contribution
+                SourcePoint32(1 * nz + 10, 2, 0.75),           # row x 1: outside the interior
+                SourcePoint32((h + 1) * nz + nz - 1, 1, 0.6),  # kz nz-2: outside the interior
+                SourcePoint32(80 * nz + 64 + 1, 2, 0.3)]       # the tile corner (x 80, z 64)
+        src = (SourcePoint32 * len(spts))(*spts)
+        ts = lib.WFD_Points_Create(ctypes.cast(src, ctypes.POINTER(SourcePoint32)), len(spts), 0)
         rec = (SourcePoint32 * len(pts))(*pts)
         tr = lib.WFD_Points_Create(ctypes.cast(rec, ctypes.POINTER(SourcePoint32)), len(pts), 1)
-        wav = torch.from_numpy(np.random.default_rng(3).standard_normal(nt).astype(np.float32)).cuda()
+        wav = torch.from_numpy(np.random.default_rng(3).standard_normal(2 * nt).astype(np.float32)).cuda()
         trc = torch.zeros(12 * nt, device="cuda")
         torch.cuda.synchronize()
         stream = ctypes.c_void_p(lib.WFD_Prop_Stream(ctypes.c_void_p(g.p)))

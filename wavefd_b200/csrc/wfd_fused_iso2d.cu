@@ -54,6 +54,61 @@ struct Tile {
     float T2[TX][T2W];
 };
 
+// Pass 1 of the tile at (x0, z0) from the pCur and B boxes in shared memory (complete and visible to
+// the CTA): the x output into T0, the z output into T2 with its symmetric image above the free
+// surface; ends with both visible to the CTA.
+__device__ __forceinline__ void pass1_tile(const Grid &g, const long x0, const long z0, Tile &sm) {
+    auto &P = sm.P;
+    auto &Bs = sm.Bs;
+    auto &T0 = sm.T0;
+    auto &T2 = sm.T2;
+    const int tz = threadIdx.x % WZ, tx = threadIdx.x / WZ;
+    // pass 1, x output (B * idx * D+x pCur) on rows x0-4 .. x0+TX+2
+#pragma unroll
+    for (int r = tx; r < T0H; r += WX) {
+#pragma unroll
+        for (int c = tz; c < TZ; c += WZ) {
+            const long x = x0 - 4 + r, z = z0 + c;
+            const int reg = region2(g, x, z);
+            float t = 0.0f;
+            if (reg) {
+                const int pr = r + 3, pc = c + 7;  // P row/column of (x, z)
+                const float dx = (reg == 2 && z == 0) ? 0.0f : g.idx * stp(g, [&](int j) { return P[pr + j][pc]; });
+                t = Bs[r][c + 4] * dx;
+            }
+            T0[r][c] = t;
+        }
+    }
+    // pass 1, z output (B * idz * D+z pCur, the image supplying kz < 0) on columns z0-4 .. z0+TZ+2
+#pragma unroll
+    for (int r = tx; r < TX; r += WX) {
+        const long x = x0 + r;
+#pragma unroll
+        for (int c = tz; c < T2W; c += WZ) {
+            const long z = z0 - 4 + c;
+            float t = 0.0f;
+            if (z >= 0) {
+                const int reg = region2(g, x, z);
+                if (reg) {
+                    const int pr = r + 7, pc = c + 3;
+                    const float dz = g.idz * stp(g, [&](int j) { return P[pr][pc + j]; });
+                    t = Bs[r + 4][c] * dz;
+                }
+            }
+            T2[r][c] = t;
+        }
+    }
+    __syncthreads();
+    if (z0 == 0) {
+        // symmetric image of the z output above the free surface: t[-j] = t[j-1] (column of kz is kz+4)
+        if (tz < 4) {
+#pragma unroll
+            for (int r = tx; r < TX; r += WX) T2[r][3 - tz] = T2[r][4 + tz];
+        }
+        __syncthreads();
+    }
+}
+
 // One step of the tile at (x0, z0): F.pcur -> F.pold, F.pspace; then the source injection F.inj at
 // time index it into the tile's cells of the new field (nothing when it is outside 1..nt). Ends with
 // the tile's writes done by every thread of the CTA only if injecting (callers reusing the shared
@@ -110,50 +165,7 @@ __device__ __forceinline__ void tile_step(const Grid &g, const Fields &F, const 
     }
     __syncthreads();
 
-    // pass 1, x output (B * idx * D+x pCur) on rows x0-4 .. x0+TX+2
-#pragma unroll
-    for (int r = tx; r < T0H; r += WX) {
-#pragma unroll
-        for (int c = tz; c < TZ; c += WZ) {
-            const long x = x0 - 4 + r, z = z0 + c;
-            const int reg = region2(g, x, z);
-            float t = 0.0f;
-            if (reg) {
-                const int pr = r + 3, pc = c + 7;  // P row/column of (x, z)
-                const float dx = (reg == 2 && z == 0) ? 0.0f : g.idx * stp(g, [&](int j) { return P[pr + j][pc]; });
-                t = Bs[r][c + 4] * dx;
-            }
-            T0[r][c] = t;
-        }
-    }
-    // pass 1, z output (B * idz * D+z pCur, the image supplying kz < 0) on columns z0-4 .. z0+TZ+2
-#pragma unroll
-    for (int r = tx; r < TX; r += WX) {
-        const long x = x0 + r;
-#pragma unroll
-        for (int c = tz; c < T2W; c += WZ) {
-            const long z = z0 - 4 + c;
-            float t = 0.0f;
-            if (z >= 0) {
-                const int reg = region2(g, x, z);
-                if (reg) {
-                    const int pr = r + 7, pc = c + 3;
-                    const float dz = g.idz * stp(g, [&](int j) { return P[pr][pc + j]; });
-                    t = Bs[r + 4][c] * dz;
-                }
-            }
-            T2[r][c] = t;
-        }
-    }
-    __syncthreads();
-    if (z0 == 0) {
-        // symmetric image of the z output above the free surface: t[-j] = t[j-1] (column of kz is kz+4)
-        if (tz < 4) {
-#pragma unroll
-            for (int r = tx; r < TX; r += WX) T2[r][3 - tz] = T2[r][4 + tz];
-        }
-        __syncthreads();
-    }
+    pass1_tile(g, x0, z0, sm);
 
     // pass 2: D-, the time update with Q, pSpace (.h:943)
 #pragma unroll
@@ -283,31 +295,182 @@ __global__ void __launch_bounds__(NT) k_iso2d_run(Grid g, Fields F, long nsteps,
         }
     }
 }
+// The whole time loop with every tile resident in one CTA (as many CTAs as tiles, all co-resident).
+// B stays in shared memory and V, Q and the tile's pOld in registers; the pCur box keeps the tile's
+// own cells from the step before (its new field), so that a step reloads only the box's ring (the
+// neighbours' cells and the free-surface image) from L2. pOld of a step is the pCur of the step
+// before, and a cell outside the interior keeps its array value (the reference does not write it),
+// so the registers and the box hold exactly what the two arrays hold. The source injection is
+// applied to the box's cells, in each group's order, before the new field is stored; the new field
+// is stored every step (the neighbours' rings and the receivers read it), pSpace only at the last
+// step, the only one whose pSpace outlives the loop. Steps, barrier and extraction as k_iso2d_run.
+constexpr int MAX_INJ = 1024;
+struct InjRef {
+    int group, cell;  // group index, cell offset in the pCur box
+};
+
+__global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long nsteps, long it0, RunExtract ex,
+                                                         unsigned *sync_words) {
+    __shared__ Tile sm;
+    __shared__ int ok_flag, n_inj;
+    __shared__ InjRef inj[MAX_INJ];
+    auto &P = sm.P;
+    auto &Bs = sm.Bs;
+    auto &T0 = sm.T0;
+    auto &T2 = sm.T2;
+    const int tz = threadIdx.x % WZ, tx = threadIdx.x / WZ;
+    const long nx = g.nx, nz = g.nz, ntz = (nz + TZ - 1) / TZ;
+    const long x0 = (long)(blockIdx.x / ntz) * TX, z0 = (long)(blockIdx.x % ntz) * TZ;
+
+    // the thread's two cells (row tx, columns tz and tz + 32): V, Q and pOld
+    float v[2] = {0.0f, 0.0f}, q[2] = {0.0f, 0.0f}, po[2] = {0.0f, 0.0f};
+    bool mine[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const long x = x0 + tx, z = z0 + tz + WZ * i;
+        mine[i] = x < nx && z < nz;
+        if (mine[i]) {
+            const long k = x * nz + z;
+            v[i] = __ldg(F.v + k);
+            q[i] = __ldg(F.q + k);
+            po[i] = __ldcg(F.pold + k);
+        }
+    }
+#pragma unroll
+    for (int r = tx; r < BXH; r += WX) {
+        const long x = x0 - 4 + r;
+#pragma unroll
+        for (int c = tz; c < BZW; c += WZ) {
+            const long z = z0 - 4 + c;
+            Bs[r][c] = (x >= 0 && x < nx && z >= 0 && z < nz) ? F.b[x * nz + z] : 0.0f;
+        }
+    }
+    // the source groups whose cell lies in this tile (tables of up to MAX_INJ groups; each group is
+    // one cell, so their order does not matter)
+    if (threadIdx.x == 0) n_inj = 0;
+    __syncthreads();
+    for (long gi = threadIdx.x; gi < F.inj.ngroups && gi < MAX_INJ; gi += NT) {
+        const long key = F.inj.key[gi];
+        const long x = key / nz, z = key - x * nz;
+        if (x >= x0 && x < x0 + TX && z >= z0 && z < z0 + TZ)
+            inj[atomicAdd(&n_inj, 1)] = InjRef{(int)gi, (int)((x - x0 + 7) * PZW + (z - z0 + 7))};
+    }
+
+    float *A = F.pcur, *B = F.pold;
+    unsigned gen = 0;
+    for (long st = 0; st < nsteps; st++) {
+        const float *pcur = (st & 1) ? B : A;
+        float *pnew = (st & 1) ? A : B;
+        const long it = it0 + st;
+        // the pCur box with its antisymmetric image above kz = 0: the whole box at the first step,
+        // afterwards the ring around the tile's own cells
+#pragma unroll
+        for (int r = tx; r < PXH; r += WX) {
+            const long x = x0 - 7 + r;
+            const bool xin = x >= 0 && x < nx, own_row = r >= 7 && r < 7 + TX;
+#pragma unroll
+            for (int c = tz; c < PZW; c += WZ) {
+                if (st > 0 && own_row && c >= 7 && c < 7 + TZ) continue;
+                const long z = z0 - 7 + c;
+                float val = 0.0f;
+                if (xin) {
+                    if (z >= 0 && z < nz) val = __ldcg(pcur + x * nz + z);
+                    else if (z < 0 && -z < nz) val = -__ldcg(pcur + x * nz - z);
+                }
+                P[r][c] = val;
+            }
+        }
+        __syncthreads();
+
+        pass1_tile(g, x0, z0, sm);
+
+        // pass 2: D-, the time update with Q (.h:943); the new field into the box's own cells
+        const bool last = st == nsteps - 1;
+        float nv[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            if (!mine[i]) continue;
+            const int r = tx, c = tz + WZ * i;
+            const long x = x0 + r, z = z0 + c;
+            const int reg = region2(g, x, z);
+            const float pc = P[r + 7][c + 7];
+            float n = po[i], L = 0.0f;
+            if (reg) {
+                float dx = 0.0f, dz = 0.0f;
+                if (!(reg == 2 && z == 0)) {
+                    dx = g.idx * stm(g, [&](int j) { return T0[r + 4 + j][c]; });
+                    dz = g.idz * stm(g, [&](int j) { return T2[r][c + 4 + j]; });
+                }
+                L = dx + dz;
+                const float dt2V2_B = g.dt2 * v[i] * v[i] / Bs[r + 4][c + 4];
+                n = dt2V2_B * L - q[i] * (pc - po[i]) - po[i] + 2 * pc;
+            }
+            if (last) F.pspace[x * nz + z] = L;
+            po[i] = pc;
+            P[r + 7][c + 7] = n;
+            nv[i] = n;
+        }
+        // the step's source injection into the new field, each group's contributions in order,
+        // separate IEEE multiply and add
+        if (n_inj && it >= 1 && it <= F.inj.nt) {
+            __syncthreads();
+            for (int li = threadIdx.x; li < n_inj; li += NT) {
+                const InjRef ref = inj[li];
+                float *cell = &P[0][0] + ref.cell;
+                float acc = *cell;
+                for (long j = F.inj.start[ref.group]; j < F.inj.start[ref.group + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(F.inj.c[j], F.inj.wav[F.inj.other[j] * F.inj.nt + (it - 1)]));
+                *cell = acc;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 2; i++) nv[i] = P[tx + 7][tz + WZ * i + 7];
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+            if (mine[i]) pnew[(x0 + tx) * nz + z0 + tz + WZ * i] = nv[i];
+
+        if (!grid_barrier(sync_words, gen, &ok_flag)) return;
+        if (ex.ngroups && it >= 1 && it <= ex.nt) {
+            for (long gi = (long)blockIdx.x * NT + threadIdx.x; gi < ex.ngroups; gi += (long)gridDim.x * NT) {
+                float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
+                float acc = *dst;
+                for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(pnew + ex.other[j])));
+                *dst = acc;
+            }
+        }
+    }
+}
 }  // namespace
 
 int iso2d_run(const Grid &g, const Fields &F, long nsteps, long it0, const RunExtract &ex, unsigned *sync_words,
               cudaStream_t s) {
     if (g.ndim != 2) return -1;
-    static int cap = 0;
-    if (!cap) {
-        int dev = 0, sms = 0, per = 0, coop = 0;
+    // co-resident CTAs of the two forms (0: the device has no cooperative launch)
+    static int cap = -1, cap_res = 0;
+    if (cap < 0) {
+        int dev = 0, sms = 0, per = 0, per_res = 0, coop = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_iso2d_run, NT, 0);
-        cap = coop && per > 0 ? sms * per : -1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_res, k_iso2d_run_res, NT, 0);
+        cap = coop ? sms * per : 0;
+        cap_res = coop ? sms * per_res : 0;
     }
-    if (cap <= 0) return -1;
     const long ntiles = ((g.nz + TZ - 1) / TZ) * ((g.nx + TX - 1) / TX);
-    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    const bool resident = ntiles <= cap_res && F.inj.ngroups <= MAX_INJ;
+    if (!resident && cap <= 0) return -1;
+    const int grid = (int)(resident ? ntiles : (ntiles < cap ? ntiles : cap));
     Grid gg = g;
     Fields FF = F;
     long ns = nsteps, i0 = it0;
     RunExtract ee = ex;
     unsigned *sw = sync_words;
     void *args[] = {&gg, &FF, &ns, &i0, &ee, &sw};
-    return cudaLaunchCooperativeKernel((const void *)k_iso2d_run, dim3(grid), dim3(NT), args, 0, s) == cudaSuccess ? 0
-                                                                                                                   : 1;
+    const void *fn = resident ? (const void *)k_iso2d_run_res : (const void *)k_iso2d_run;
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), args, 0, s) == cudaSuccess ? 0 : 1;
 }
 
 bool fused_iso2d(const Grid &g, const Fields &F, cudaStream_t s) {
