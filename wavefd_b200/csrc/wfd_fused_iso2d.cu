@@ -303,7 +303,9 @@ __global__ void __launch_bounds__(NT) k_iso2d_run(Grid g, Fields F, long nsteps,
 // so the registers and the box hold exactly what the two arrays hold. The source injection is
 // applied to the box's cells, in each group's order, before the new field is stored; the new field
 // is stored every step (the neighbours' rings and the receivers read it), pSpace only at the last
-// step, the only one whose pSpace outlives the loop. Steps, barrier and extraction as k_iso2d_run.
+// step, the only one whose pSpace outlives the loop. The receivers of a step read its new field after
+// the barrier, with the next step's ring loads (the last step's after the loop); barrier as
+// k_iso2d_run.
 constexpr int MAX_INJ = 1024;
 struct InjRef {
     int group, cell;  // group index, cell offset in the pCur box
@@ -314,6 +316,7 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
     __shared__ Tile sm;
     __shared__ int ok_flag, n_inj;
     __shared__ InjRef inj[MAX_INJ];
+    __shared__ float Qs[TX][TZ], Ds[TX][TZ];
     auto &P = sm.P;
     auto &Bs = sm.Bs;
     auto &T0 = sm.T0;
@@ -322,20 +325,9 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
     const long nx = g.nx, nz = g.nz, ntz = (nz + TZ - 1) / TZ;
     const long x0 = (long)(blockIdx.x / ntz) * TX, z0 = (long)(blockIdx.x % ntz) * TZ;
 
-    // the thread's two cells (row tx, columns tz and tz + 32): V, Q and pOld
-    float v[2] = {0.0f, 0.0f}, q[2] = {0.0f, 0.0f}, po[2] = {0.0f, 0.0f};
-    bool mine[2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        const long x = x0 + tx, z = z0 + tz + WZ * i;
-        mine[i] = x < nx && z < nz;
-        if (mine[i]) {
-            const long k = x * nz + z;
-            v[i] = __ldg(F.v + k);
-            q[i] = __ldg(F.q + k);
-            po[i] = __ldcg(F.pold + k);
-        }
-    }
+    // B over the box; the thread's two cells (row tx, columns tz and tz + 32): pOld in registers,
+    // Q and dt^2 V^2 / B (the same operations, in the same order, as every step would repeat) in
+    // shared memory
 #pragma unroll
     for (int r = tx; r < BXH; r += WX) {
         const long x = x0 - 4 + r;
@@ -343,6 +335,20 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
         for (int c = tz; c < BZW; c += WZ) {
             const long z = z0 - 4 + c;
             Bs[r][c] = (x >= 0 && x < nx && z >= 0 && z < nz) ? F.b[x * nz + z] : 0.0f;
+        }
+    }
+    float po[2] = {0.0f, 0.0f};
+    bool mine[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const long x = x0 + tx, z = z0 + tz + WZ * i;
+        mine[i] = x < nx && z < nz;
+        if (mine[i]) {
+            const long k = x * nz + z;
+            const float V = __ldg(F.v + k);
+            Qs[tx][tz + WZ * i] = __ldg(F.q + k);
+            Ds[tx][tz + WZ * i] = g.dt2 * V * V / F.b[k];
+            po[i] = __ldcg(F.pold + k);
         }
     }
     // the source groups whose cell lies in this tile (tables of up to MAX_INJ groups; each group is
@@ -356,28 +362,89 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
             inj[atomicAdd(&n_inj, 1)] = InjRef{(int)gi, (int)((x - x0 + 7) * PZW + (z - z0 + 7))};
     }
 
+    // the receiver groups of this thread (group blockIdx.x + threadIdx.x * CTAs, and every CTAs x NT
+    // after it), the first one's description in registers: a group of one point, the common case,
+    // has its two loads issued with the step's ring loads
+    const long G = gridDim.x, egi = blockIdx.x + (long)threadIdx.x * G;
+    const bool emine = egi < ex.ngroups;
+    float *edst = nullptr;  // the group's trace, at time index 1
+    long eoth = -1;         // the single point's cell, -1 for a group of several points
+    float ec = 0.0f;
+    if (emine) {
+        edst = ex.data + ex.key[egi] * ex.nt;
+        const long j0 = ex.start[egi];
+        if (ex.start[egi + 1] - j0 == 1) {
+            eoth = ex.other[j0];
+            ec = ex.c[j0];
+        }
+    }
+
     float *A = F.pcur, *B = F.pold;
     unsigned gen = 0;
-    for (long st = 0; st < nsteps; st++) {
+    for (long st = 0;; st++) {
+        // pCur of step st is the new field of step st - 1, which the receivers read
         const float *pcur = (st & 1) ? B : A;
         float *pnew = (st & 1) ? A : B;
-        const long it = it0 + st;
-        // the pCur box with its antisymmetric image above kz = 0: the whole box at the first step,
-        // afterwards the ring around the tile's own cells
+        const long it = it0 + st, ite = it - 1;
+        const bool exs = st > 0 && ex.ngroups && ite >= 1 && ite <= ex.nt;
+        float ed = 0.0f, ef = 0.0f;
+        if (exs && emine) {
+            ed = edst[ite - 1];
+            if (eoth >= 0) ef = __ldcg(pcur + eoth);
+        }
+        // the pCur box with its antisymmetric image above kz = 0, into registers: the whole box at the
+        // first step, afterwards the ring around the tile's own cells; the corners (outside the
+        // tile's rows and its columns) are never read
+        float rv[2][3];
+        const bool ring = st < nsteps;
 #pragma unroll
-        for (int r = tx; r < PXH; r += WX) {
+        for (int ri = 0; ri < 2; ri++) {
+            const int r = tx + WX * ri;
             const long x = x0 - 7 + r;
             const bool xin = x >= 0 && x < nx, own_row = r >= 7 && r < 7 + TX;
 #pragma unroll
-            for (int c = tz; c < PZW; c += WZ) {
-                if (st > 0 && own_row && c >= 7 && c < 7 + TZ) continue;
+            for (int ci = 0; ci < 3; ci++) {
+                const int c = tz + WZ * ci;
+                const bool own_col = c >= 7 && c < 7 + TZ;
                 const long z = z0 - 7 + c;
                 float val = 0.0f;
-                if (xin) {
+                if (ring && r < PXH && c < PZW && (own_row != own_col || (st == 0 && own_row)) && xin) {
                     if (z >= 0 && z < nz) val = __ldcg(pcur + x * nz + z);
                     else if (z < 0 && -z < nz) val = -__ldcg(pcur + x * nz - z);
                 }
-                P[r][c] = val;
+                rv[ri][ci] = val;
+            }
+        }
+        // the extraction of step st - 1: data[key*nt + it-1] += sum c * field[other], each group in
+        // order, IEEE multiply and add
+        if (exs) {
+            if (emine) {
+                float acc = ed;
+                if (eoth >= 0)
+                    acc = __fadd_rn(acc, __fmul_rn(ec, ef));
+                else
+                    for (long j = ex.start[egi]; j < ex.start[egi + 1]; j++)
+                        acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(pcur + ex.other[j])));
+                edst[ite - 1] = acc;
+            }
+            for (long gi = egi + G * NT; gi < ex.ngroups; gi += G * NT) {
+                float *dst = ex.data + ex.key[gi] * ex.nt + (ite - 1);
+                float acc = *dst;
+                for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(pcur + ex.other[j])));
+                *dst = acc;
+            }
+        }
+        if (!ring) break;
+#pragma unroll
+        for (int ri = 0; ri < 2; ri++) {
+            const int r = tx + WX * ri;
+            const bool own_row = r >= 7 && r < 7 + TX;
+#pragma unroll
+            for (int ci = 0; ci < 3; ci++) {
+                const int c = tz + WZ * ci;
+                const bool own_col = c >= 7 && c < 7 + TZ;
+                if (r < PXH && c < PZW && (own_row != own_col || (st == 0 && own_row))) P[r][c] = rv[ri][ci];
             }
         }
         __syncthreads();
@@ -402,8 +469,7 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
                     dz = g.idz * stm(g, [&](int j) { return T2[r][c + 4 + j]; });
                 }
                 L = dx + dz;
-                const float dt2V2_B = g.dt2 * v[i] * v[i] / Bs[r + 4][c + 4];
-                n = dt2V2_B * L - q[i] * (pc - po[i]) - po[i] + 2 * pc;
+                n = Ds[r][c] * L - Qs[r][c] * (pc - po[i]) - po[i] + 2 * pc;
             }
             if (last) F.pspace[x * nz + z] = L;
             po[i] = pc;
@@ -431,15 +497,6 @@ __global__ void __launch_bounds__(NT, 2) k_iso2d_run_res(Grid g, Fields F, long 
             if (mine[i]) pnew[(x0 + tx) * nz + z0 + tz + WZ * i] = nv[i];
 
         if (!grid_barrier(sync_words, gen, &ok_flag)) return;
-        if (ex.ngroups && it >= 1 && it <= ex.nt) {
-            for (long gi = (long)blockIdx.x * NT + threadIdx.x; gi < ex.ngroups; gi += (long)gridDim.x * NT) {
-                float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
-                float acc = *dst;
-                for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
-                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(pnew + ex.other[j])));
-                *dst = acc;
-            }
-        }
     }
 }
 }  // namespace
