@@ -84,19 +84,15 @@ struct K {
         if (strict) wfd_strict::fn(a...);                                     \
         else wfd_fast::fn(a...);                                              \
     }
-    WFD_DISPATCH(dplus)
-    WFD_DISPATCH(dminus3)
-    WFD_DISPATCH(tti_dplus)
-    WFD_DISPATCH(tti_dminus)
     WFD_DISPATCH(born_iso)
-    WFD_DISPATCH(born_iso_scaleb)
     WFD_DISPATCH(born_aniso_v)
-    WFD_DISPATCH(born_vea_sandwich)
-    WFD_DISPATCH(born_vea_final)
     WFD_DISPATCH(image_iso)
     WFD_DISPATCH(image_aniso_v)
-    WFD_DISPATCH(image_vea)
     WFD_DISPATCH(image_wavefieldsep)
+    WFD_DISPATCH(born_iso_fused)
+    WFD_DISPATCH(image_iso_fused)
+    WFD_DISPATCH(born_vea_fused)
+    WFD_DISPATCH(image_vea_fused)
 #undef WFD_DISPATCH
 };
 
@@ -105,12 +101,6 @@ int finish(Prop *p, const char *what) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) return prop_fail(p, WFD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     return WFD_OK;
-}
-
-// gradient triple for the VEA helpers: plain D+ for VTI, rotated D+ for TTI
-void vea_grad(const K &k, Prop *p, const Grid &g, const Fields &F, const float *in, float *const *o) {
-    if (p->phys == TTI) k.tti_dplus(g, F, in, o[0], o[1], o[2], p->stream);
-    else k.dplus(g, in, o[0], o[1], o[2], p->stream);
 }
 
 }  // namespace
@@ -130,28 +120,14 @@ int prop_born(Prop *p, const char *variant, float *const *args, int nargs) {
         } else {
             const bool vb = !strcmp(variant, "VB");
             float *dv = vb ? a[0] : nullptr, *db = vb ? a[1] : a[0], *P = vb ? a[2] : a[1], *DP = vb ? a[3] : a[2];
-            if (!ensure_scratch(p, 6)) return p->status;
-            k.dplus(g, P, t[0], t[1], t[2], p->stream);
-            k.born_iso_scaleb(g, db, (const float *const *)t, t + 3, p->stream);
-            k.dminus3(g, t[3], t[4], t[5], t[0], t[1], t[2], p->stream);
-            k.born_iso(g, vb ? 1 : 2, F, dv, db, DP, (const float *const *)t, p->stream);
+            if (!ensure_scratch(p, 3)) return p->status;
+            k.born_iso_fused(g, vb ? 1 : 2, F, dv, db, P, DP, t, p->stream);
         }
     } else if (!strcmp(variant, "V")) {
         k.born_aniso_v(g, F, a[0], a[1], a[2], p->stream);
     } else {  // VEA: dV, dEps, dEta, P, M, DP, DM
-        if (!ensure_scratch(p, 12)) return p->status;
-        vea_grad(k, p, g, F, a[3], t);
-        vea_grad(k, p, g, F, a[4], t + 3);
-        k.born_vea_sandwich(g, F, a[1], a[2], (const float *const *)t, (const float *const *)(t + 3), t + 6, t + 9,
-                            p->stream);
-        if (p->phys == TTI) {
-            k.tti_dminus(g, F, t[6], t[7], t[8], t[0], t[1], t[2], p->stream);
-            k.tti_dminus(g, F, t[9], t[10], t[11], t[3], t[4], t[5], p->stream);
-        } else {
-            k.dminus3(g, t[6], t[7], t[8], t[0], t[1], t[2], p->stream);
-            k.dminus3(g, t[9], t[10], t[11], t[3], t[4], t[5], p->stream);
-        }
-        k.born_vea_final(g, F, a[0], a[5], a[6], (const float *const *)t, (const float *const *)(t + 3), p->stream);
+        if (!ensure_scratch(p, 6)) return p->status;
+        k.born_vea_fused(g, p->phys == TTI, F, a[0], a[1], a[2], a[3], a[4], a[5], a[6], t, p->stream);
     }
     return finish(p, "ForwardBornInjection");
 }
@@ -186,11 +162,7 @@ int prop_image(Prop *p, const char *variant, float *const *args, int nargs, long
         } else {
             const bool vb = !strcmp(variant, "VB");
             float *dv = vb ? a[0] : nullptr, *db = vb ? a[1] : a[0], *P = vb ? a[2] : a[1], *DP = vb ? a[3] : a[2];
-            if (!ensure_scratch(p, 6)) return p->status;
-            k.dplus(g, P, t[0], t[1], t[2], p->stream);
-            k.dplus(g, F.pold, t[3], t[4], t[5], p->stream);
-            k.image_iso(g, vb ? 1 : 2, F, DP, (const float *const *)t, (const float *const *)(t + 3), dv, db,
-                        p->stream);
+            k.image_iso_fused(g, vb ? 1 : 2, F, DP, P, dv, db, p->stream);
             if (dv) outs.push_back(dv);
             outs.push_back(db);
         }
@@ -198,13 +170,7 @@ int prop_image(Prop *p, const char *variant, float *const *args, int nargs, long
         k.image_aniso_v(g, F, a[1], a[2], a[0], p->stream);
         outs.push_back(a[0]);
     } else {  // VEA: dV, dEps, dEta, P, M, DP, DM
-        if (!ensure_scratch(p, 12)) return p->status;
-        vea_grad(k, p, g, F, a[3], t);
-        vea_grad(k, p, g, F, a[4], t + 3);
-        vea_grad(k, p, g, F, F.pold, t + 6);
-        vea_grad(k, p, g, F, F.mold, t + 9);
-        k.image_vea(g, F, a[5], a[6], (const float *const *)t, (const float *const *)(t + 3),
-                    (const float *const *)(t + 6), (const float *const *)(t + 9), a[0], a[1], a[2], p->stream);
+        k.image_vea_fused(g, p->phys == TTI, F, a[5], a[6], a[3], a[4], a[0], a[1], a[2], p->stream);
         outs.push_back(a[0]);
         outs.push_back(a[1]);
         outs.push_back(a[2]);

@@ -282,85 +282,14 @@ __global__ void __launch_bounds__(kThreads) k_dplus(Grid g, const float *__restr
     oz[k] = dz;
 }
 
-__global__ void __launch_bounds__(kThreads) k_dminus3(Grid g, const float *__restrict__ fx,
-                                                      const float *__restrict__ fy, const float *__restrict__ fz,
-                                                      float *ox, float *oy, float *oz) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    long x, y, z;
-    cell_xyz(g, k, x, y, z);
-    const int r = region(g, x, y, z);
-    float dx = 0.0f, dy = 0.0f, dz = 0.0f;
-    if (r) gradm3(g, fx, fy, fz, k, z, r, dx, dy, dz);
-    ox[k] = dx;
-    if (g.ndim == 3) oy[k] = dy;
-    oz[k] = dz;
-}
-
-// rotated D+ of the TTI Born/imaging helpers (3D .h:2910-3166; 2D .h:1366-1530)
-__global__ void __launch_bounds__(kThreads) k_tti_dplus(Grid g, Fields F, const float *__restrict__ in, float *o1,
-                                                        float *o2, float *o3) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    long x, y, z;
-    cell_xyz(g, k, x, y, z);
-    const int r = region(g, x, y, z);
-    if (!r) {
-        o1[k] = 0.0f;
-        if (g.ndim == 3) o2[k] = 0.0f;
-        o3[k] = 0.0f;
-        return;
-    }
-    float dx, dy, dz;
-    gradp(g, in, k, z, r, dx, dy, dz);
-    const float st = F.st[k], ct = F.ct[k];
-    if (g.ndim == 3) {
-        const float sp = F.sp[k], cp = F.cp[k];
-        const float cosThetaCosPhi = ct * cp;
-        const float cosThetaSinPhi = ct * sp;
-        const float sinThetaCosPhi = st * cp;
-        o1[k] = cosThetaCosPhi * dx + cosThetaSinPhi * dy - st * dz;
-        o2[k] = -sp * dx + cp * dy;
-        o3[k] = sinThetaCosPhi * dx + st * sp * dy + ct * dz;
-    } else {
-        o1[k] = ct * dx - st * dz;
-        o3[k] = st * dx + ct * dz;
-    }
-}
-
-// rotated D- with the back-rotation inside the stencil (3D .h:3171-3661; 2D .h:1531-1719)
-__global__ void __launch_bounds__(kThreads) k_tti_dminus(Grid g, Fields F, const float *__restrict__ i1,
-                                                         const float *__restrict__ i2, const float *__restrict__ i3,
-                                                         float *o1, float *o2, float *o3) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    long x, y, z;
-    cell_xyz(g, k, x, y, z);
-    const int r = region(g, x, y, z);
-    if (!r || (r == 2 && z == 0)) {
-        o1[k] = 0.0f;
-        if (g.ndim == 3) o2[k] = 0.0f;
-        o3[k] = 0.0f;
-        return;
-    }
-    const long k0 = k - z;
-    if (g.ndim == 3) {
-        o1[k] = g.idx * stm_t(g, T2{F.ct, F.cp, i1}, k, g.sx) + g.idy * stm_t(g, T2{F.ct, F.sp, i1}, k, g.sy) -
-                g.idz * stmz_t(g, T1{F.st, i1}, k0, z);
-        o2[k] = -g.idx * stm_t(g, T1{F.sp, i2}, k, g.sx) + g.idy * stm_t(g, T1{F.cp, i2}, k, g.sy);
-        o3[k] = g.idx * stm_t(g, T2{F.st, F.cp, i3}, k, g.sx) + g.idy * stm_t(g, T2{F.st, F.sp, i3}, k, g.sy) +
-                g.idz * stmz_t(g, T1{F.ct, i3}, k0, z);
-    } else {
-        o1[k] = g.idx * stm_t(g, T1{F.ct, i1}, k, g.sx) - g.idz * stmz_t(g, T1{F.st, i1}, k0, z);
-        o3[k] = g.idx * stm_t(g, T1{F.st, i3}, k, g.sx) + g.idz * stmz_t(g, T1{F.ct, i3}, k0, z);
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // Born injection. Iso V: 3D .h:305-334, 2D .h:253-280 (a different expression);
 // Iso VB/B final loops: 3D .h:389-416 / .h:471-497 and the 2D forms.
 struct Ptr3 {
     const float *p[3];
+};
+struct MPtr3 {
+    float *p[3];
 };
 __global__ void __launch_bounds__(kThreads) k_born_iso(Grid g, int which, Fields F, const float *__restrict__ dv,
                                                        const float *__restrict__ db, const float *__restrict__ dp,
@@ -405,20 +334,6 @@ __global__ void __launch_bounds__(kThreads) k_born_iso(Grid g, int which, Fields
     }
 }
 
-// tmpP2 = dB * tmpP1 (3D Iso .h:369-373)
-struct MPtr3 {
-    float *p[3];
-};
-__global__ void __launch_bounds__(kThreads) k_born_iso_scaleb(Grid g, const float *__restrict__ db, Ptr3 t1,
-                                                              MPtr3 t2) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    const float dB = db[k];
-    t2.p[0][k] = dB * t1.p[0][k];
-    if (g.ndim == 3) t2.p[1][k] = dB * t1.p[1][k];
-    t2.p[2][k] = dB * t1.p[2][k];
-}
-
 // Born injection V for VTI/TTI (3D VTI .h:420-452; 3D TTI .h:423-452; 2D alike)
 __global__ void __launch_bounds__(kThreads) k_born_aniso_v(Grid g, Fields F, const float *__restrict__ dv,
                                                            const float *__restrict__ dp,
@@ -429,39 +344,6 @@ __global__ void __launch_bounds__(kThreads) k_born_aniso_v(Grid g, Fields F, con
     const float factor = 2 * g.dt * g.dt * dV / V;
     F.pcur[k] += factor * dp[k];
     F.mcur[k] += factor * dm[k];
-}
-
-// VEA sandwich (3D VTI .h:499-511; 3D TTI .h:500-512; 2D VTI/TTI alike)
-__global__ void __launch_bounds__(kThreads) k_born_vea_sandwich(Grid g, Fields F, const float *__restrict__ de,
-                                                                const float *__restrict__ da, Ptr3 tp1, Ptr3 tm1,
-                                                                MPtr3 tp2, MPtr3 tm2) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    const float A = F.eta[k], B = F.b[k], Fv = F.f[k], dE = de[k], dA = da[k];
-    tp2.p[0][k] = (+2 * B * dE) * tp1.p[0][k];
-    if (g.ndim == 3) tp2.p[1][k] = (+2 * B * dE) * tp1.p[1][k];
-    tp2.p[2][k] = (-2 * B * Fv * A * dA) * tp1.p[2][k] + (dA * B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tm1.p[2][k];
-    tm2.p[0][k] = 0.0f;
-    if (g.ndim == 3) tm2.p[1][k] = 0.0f;
-    tm2.p[2][k] = (+2 * B * Fv * A * dA) * tm1.p[2][k] + (dA * B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tp1.p[2][k];
-}
-
-// VEA final update (3D VTI .h:533-548; 3D TTI .h:536-551; 2D alike)
-__global__ void __launch_bounds__(kThreads) k_born_vea_final(Grid g, Fields F, const float *__restrict__ dv,
-                                                             const float *__restrict__ dp,
-                                                             const float *__restrict__ dm, Ptr3 lp, Ptr3 lm) {
-    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= g.n) return;
-    const float V = F.v[k], B = F.b[k], dV = dv[k];
-    const float dt2v2OverB = g.dt * g.dt * V * V / B;
-    const float factor = 2 * B * dV / (V * V * V);
-    if (g.ndim == 3) {
-        F.pcur[k] += dt2v2OverB * (factor * dp[k] + lp.p[0][k] + lp.p[1][k] + lp.p[2][k]);
-        F.mcur[k] += dt2v2OverB * (factor * dm[k] + lm.p[0][k] + lm.p[1][k] + lm.p[2][k]);
-    } else {
-        F.pcur[k] += dt2v2OverB * (factor * dp[k] + lp.p[0][k] + lp.p[2][k]);
-        F.mcur[k] += dt2v2OverB * (factor * dm[k] + lm.p[0][k] + lm.p[2][k]);
-    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -495,24 +377,228 @@ __global__ void __launch_bounds__(kThreads) k_image_aniso_v(Grid g, Fields F, co
     dv[k] += factor * (dp[k] * F.pold[k] + dm[k] * F.mold[k]);
 }
 
-// VEA (3D VTI .h:730-787; 3D TTI .h:733-790; 2D VTI .h:629-690; 2D TTI alike)
-__global__ void __launch_bounds__(kThreads) k_image_vea(Grid g, Fields F, const float *__restrict__ dp,
-                                                        const float *__restrict__ dm, Ptr3 tp1, Ptr3 tm1, Ptr3 tp2,
-                                                        Ptr3 tm2, float *dv, float *de, float *da) {
+
+// ---------------------------------------------------------------------------------------------
+// The VB/B and VEA Born injections and imaging conditions: the gradient triples and their D- are
+// formed per cell in registers, not passed through scratch arrays (the reference's tmp arrays),
+// each value by the reference's operations (applyFirstDerivatives3D_PlusHalf / MinusHalf,
+// propagatorStaticFunctions.h:10-738, and the rotated forms of the TTI helpers, 3D TTI
+// .h:2910-3661, 2D .h:1366-1719). Born VB/B: 2 launches and 3 scratch arrays
+// (from 4 launches and 6); Born VEA: 2 launches and 6 (from 6 and 12); imaging VB/B and VEA: 1
+// launch and no scratch (from 3 and 5).
+
+// gradient triple at cell k, zero outside the interior: D+ (as k_dplus writes it) or, rotated, its
+// TTI form (3D .h:2910-3166; 2D .h:1366-1530); 2D leaves o[1] zero
+template <bool ROT>
+__device__ __forceinline__ void grad_at(const Grid &g, const Fields &F, const float *__restrict__ in, long k, long z,
+                                        int r, float (&o)[3]) {
+    o[0] = 0.0f;
+    o[1] = 0.0f;
+    o[2] = 0.0f;
+    if (!r) return;
+    float dx, dy, dz;
+    gradp(g, in, k, z, r, dx, dy, dz);
+    if (!ROT) {
+        o[0] = dx;
+        o[1] = dy;
+        o[2] = dz;
+        return;
+    }
+    const float st = F.st[k], ct = F.ct[k];
+    if (g.ndim == 3) {
+        const float sp = F.sp[k], cp = F.cp[k];
+        const float cosThetaCosPhi = ct * cp;
+        const float cosThetaSinPhi = ct * sp;
+        const float sinThetaCosPhi = st * cp;
+        o[0] = cosThetaCosPhi * dx + cosThetaSinPhi * dy - st * dz;
+        o[1] = -sp * dx + cp * dy;
+        o[2] = sinThetaCosPhi * dx + st * sp * dy + ct * dz;
+    } else {
+        o[0] = ct * dx - st * dz;
+        o[2] = st * dx + ct * dz;
+    }
+}
+
+// D- triple at cell k, zero outside the interior and on kz = 0 under a free surface: plain, or
+// rotated with the back-rotation inside the stencil (3D .h:3171-3661; 2D .h:1531-1719)
+template <bool ROT>
+__device__ __forceinline__ void dminus_at(const Grid &g, const Fields &F, const float *__restrict__ i1,
+                                          const float *__restrict__ i2, const float *__restrict__ i3, long k, long z,
+                                          int r, float (&o)[3]) {
+    o[0] = 0.0f;
+    o[1] = 0.0f;
+    o[2] = 0.0f;
+    if (!ROT) {
+        if (r) gradm3(g, i1, i2, i3, k, z, r, o[0], o[1], o[2]);
+        return;
+    }
+    if (!r || (r == 2 && z == 0)) return;
+    const long k0 = k - z;
+    if (g.ndim == 3) {
+        o[0] = g.idx * stm_t(g, T2{F.ct, F.cp, i1}, k, g.sx) + g.idy * stm_t(g, T2{F.ct, F.sp, i1}, k, g.sy) -
+               g.idz * stmz_t(g, T1{F.st, i1}, k0, z);
+        o[1] = -g.idx * stm_t(g, T1{F.sp, i2}, k, g.sx) + g.idy * stm_t(g, T1{F.cp, i2}, k, g.sy);
+        o[2] = g.idx * stm_t(g, T2{F.st, F.cp, i3}, k, g.sx) + g.idy * stm_t(g, T2{F.st, F.sp, i3}, k, g.sy) +
+               g.idz * stmz_t(g, T1{F.ct, i3}, k0, z);
+    } else {
+        o[0] = g.idx * stm_t(g, T1{F.ct, i1}, k, g.sx) - g.idz * stmz_t(g, T1{F.st, i1}, k0, z);
+        o[2] = g.idx * stm_t(g, T1{F.st, i3}, k, g.sx) + g.idz * stmz_t(g, T1{F.ct, i3}, k0, z);
+    }
+}
+
+// Born VB/B, first launch: t = dB * D+ P (3D Iso .h:353-381)
+__global__ void __launch_bounds__(kThreads) k_born_iso_b1(Grid g, Fields F, const float *__restrict__ db,
+                                                          const float *__restrict__ P, MPtr3 t) {
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    float d[3];
+    grad_at<false>(g, F, P, k, z, region(g, x, y, z), d);
+    const float dB = db[k];
+    t.p[0][k] = dB * d[0];
+    if (g.ndim == 3) t.p[1][k] = dB * d[1];
+    t.p[2][k] = dB * d[2];
+}
+
+// Born VB/B, second launch: D- of t and the update of pCur (3D .h:383-416 / .h:466-497; 2D alike)
+__global__ void __launch_bounds__(kThreads) k_born_iso_b2(Grid g, int which, Fields F, const float *__restrict__ dv,
+                                                          const float *__restrict__ db, const float *__restrict__ dp,
+                                                          Ptr3 t) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    float L[3];
+    dminus_at<false>(g, F, t.p[0], t.p[1], t.p[2], k, z, region(g, x, y, z), L);
+    const float V = F.v[k], B = F.b[k];
+    const float dt = g.dt;
+    const float dB = db[k];
+    if (g.ndim == 3) {
+        const float dt2v2OverB = dt * dt * V * V / B;
+        const float factorB = -dB / (V * V);
+        if (which == 1) {
+            const float dV = dv[k];
+            const float factorV = 2 * B * dV / (V * V * V);
+            F.pcur[k] += dt2v2OverB * (dp[k] * (factorV + factorB) + L[0] + L[1] + L[2]);
+        } else {
+            F.pcur[k] += dt2v2OverB * (dp[k] * factorB + L[0] + L[1] + L[2]);
+        }
+    } else {
+        const float V2 = V * V;
+        const float dt2v2OverB = dt * dt * V2 / B;
+        if (which == 1) {
+            const float dV = dv[k];
+            F.pcur[k] += dt2v2OverB * (dp[k] / V2 * (2 * B * dV / V - dB) + L[0] + L[2]);
+        } else {
+            const float factorB = -dB / V2;
+            F.pcur[k] += dt2v2OverB * (dp[k] * factorB + L[0] + L[2]);
+        }
+    }
+}
+
+// imaging VB/B in one launch: D+ of P and of pOld at the cell (3D Iso .h:563-656; 2D alike)
+__global__ void __launch_bounds__(kThreads) k_image_iso_b(Grid g, int which, Fields F, const float *__restrict__ dp,
+                                                          const float *__restrict__ P, float *dv, float *db) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    const int r = region(g, x, y, z);
+    float a[3], b[3];
+    grad_at<false>(g, F, P, k, z, r, a);
+    grad_at<false>(g, F, F.pold, k, z, r, b);
+    const float V = F.v[k], B = F.b[k];
+    const float po = F.pold[k];
+    if (which == 1) {
+        const float factorV = +2 * B / (V * V * V);
+        dv[k] += factorV * dp[k] * po;
+    }
+    const float factorB = -1 / (V * V);
+    if (g.ndim == 3)
+        db[k] += factorB * dp[k] * po - a[0] * b[0] - a[1] * b[1] - a[2] * b[2];
+    else
+        db[k] += factorB * dp[k] * po - a[0] * b[0] - a[2] * b[2];
+}
+
+// Born VEA, first launch: the gradient triples of P and M and the sandwich into tp2, tm2 (3D VTI
+// .h:480-511; 3D TTI .h:481-512; 2D alike)
+template <bool ROT>
+__global__ void __launch_bounds__(kThreads) k_born_vea_1(Grid g, Fields F, const float *__restrict__ de,
+                                                         const float *__restrict__ da, const float *__restrict__ P,
+                                                         const float *__restrict__ M, MPtr3 tp2, MPtr3 tm2) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    const int r = region(g, x, y, z);
+    float tp1[3], tm1[3];
+    grad_at<ROT>(g, F, P, k, z, r, tp1);
+    grad_at<ROT>(g, F, M, k, z, r, tm1);
+    const float A = F.eta[k], B = F.b[k], Fv = F.f[k], dE = de[k], dA = da[k];
+    tp2.p[0][k] = (+2 * B * dE) * tp1[0];
+    if (g.ndim == 3) tp2.p[1][k] = (+2 * B * dE) * tp1[1];
+    tp2.p[2][k] = (-2 * B * Fv * A * dA) * tp1[2] + (dA * B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tm1[2];
+    tm2.p[0][k] = 0.0f;
+    if (g.ndim == 3) tm2.p[1][k] = 0.0f;
+    tm2.p[2][k] = (+2 * B * Fv * A * dA) * tm1[2] + (dA * B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tp1[2];
+}
+
+// Born VEA, second launch: D- of tp2 and tm2 and the update of pCur, mCur (3D VTI .h:513-548;
+// 3D TTI .h:514-551; 2D alike)
+template <bool ROT>
+__global__ void __launch_bounds__(kThreads) k_born_vea_2(Grid g, Fields F, const float *__restrict__ dv,
+                                                         const float *__restrict__ dp, const float *__restrict__ dm,
+                                                         Ptr3 tp2, Ptr3 tm2) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    const int r = region(g, x, y, z);
+    float lp[3], lm[3];
+    dminus_at<ROT>(g, F, tp2.p[0], tp2.p[1], tp2.p[2], k, z, r, lp);
+    dminus_at<ROT>(g, F, tm2.p[0], tm2.p[1], tm2.p[2], k, z, r, lm);
+    const float V = F.v[k], B = F.b[k], dV = dv[k];
+    const float dt2v2OverB = g.dt * g.dt * V * V / B;
+    const float factor = 2 * B * dV / (V * V * V);
+    if (g.ndim == 3) {
+        F.pcur[k] += dt2v2OverB * (factor * dp[k] + lp[0] + lp[1] + lp[2]);
+        F.mcur[k] += dt2v2OverB * (factor * dm[k] + lm[0] + lm[1] + lm[2]);
+    } else {
+        F.pcur[k] += dt2v2OverB * (factor * dp[k] + lp[0] + lp[2]);
+        F.mcur[k] += dt2v2OverB * (factor * dm[k] + lm[0] + lm[2]);
+    }
+}
+
+// imaging VEA in one launch: the gradient triples of P, M, pOld and mOld at the cell (3D VTI
+// .h:730-787; 3D TTI .h:733-790; 2D alike)
+template <bool ROT>
+__global__ void __launch_bounds__(kThreads) k_image_vea_f(Grid g, Fields F, const float *__restrict__ dp,
+                                                          const float *__restrict__ dm, const float *__restrict__ P,
+                                                          const float *__restrict__ M, float *dv, float *de,
+                                                          float *da) {
+    const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n) return;
+    long x, y, z;
+    cell_xyz(g, k, x, y, z);
+    const int r = region(g, x, y, z);
+    float tp1[3], tm1[3], tp2[3], tm2[3];
+    grad_at<ROT>(g, F, P, k, z, r, tp1);
+    grad_at<ROT>(g, F, M, k, z, r, tm1);
+    grad_at<ROT>(g, F, F.pold, k, z, r, tp2);
+    grad_at<ROT>(g, F, F.mold, k, z, r, tm2);
     const float V = F.v[k], A = F.eta[k], B = F.b[k], Fv = F.f[k];
     const float factor = 2 * B / (V * V * V);
     if (g.ndim == 3) {
         dv[k] += factor * (dp[k] * F.pold[k] + dm[k] * F.mold[k]);
-        de[k] += (-2 * B * tp1.p[0][k] * tp2.p[0][k] - 2 * B * tp1.p[1][k] * tp2.p[1][k]);
+        de[k] += (-2 * B * tp1[0] * tp2[0] - 2 * B * tp1[1] * tp2[1]);
     } else {
         dv[k] += factor * dp[k] * F.pold[k] + factor * dm[k] * F.mold[k];
-        de[k] += -2 * B * tp1.p[0][k] * tp2.p[0][k];
+        de[k] += -2 * B * tp1[0] * tp2[0];
     }
-    const float partP = 2 * B * Fv * A * tp1.p[2][k] - (B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tm1.p[2][k];
-    const float partM = 2 * B * Fv * A * tm1.p[2][k] + (B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tp1.p[2][k];
-    da[k] += (partP * tp2.p[2][k] - partM * tm2.p[2][k]);
+    const float partP = 2 * B * Fv * A * tp1[2] - (B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tm1[2];
+    const float partM = 2 * B * Fv * A * tm1[2] + (B * Fv * (1 - 2 * A * A) / sqrtf(1 - A * A)) * tp1[2];
+    da[k] += (partP * tp2[2] - partM * tm2[2]);
 }
 
 Ptr3 p3(const float *const *a) { return Ptr3{{a[0], a[1], a[2]}}; }
@@ -540,27 +626,9 @@ void scale(const Grid &g, const Fields &F, bool two, cudaStream_t s) {
     k_scale<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, two ? 1 : 0);
 }
 
-void dplus(const Grid &g, const float *in, float *ox, float *oy, float *oz, cudaStream_t s) {
-    k_dplus<<<blocks_for(g.n), kThreads, 0, s>>>(g, in, in, in, ox, oy, oz);
-}
-
 void dplus3(const Grid &g, const float *inx, const float *iny, const float *inz, float *ox, float *oy, float *oz,
             cudaStream_t s) {
     k_dplus<<<blocks_for(g.n), kThreads, 0, s>>>(g, inx, iny, inz, ox, oy, oz);
-}
-
-void dminus3(const Grid &g, const float *fx, const float *fy, const float *fz, float *ox, float *oy, float *oz,
-             cudaStream_t s) {
-    k_dminus3<<<blocks_for(g.n), kThreads, 0, s>>>(g, fx, fy, fz, ox, oy, oz);
-}
-
-void tti_dplus(const Grid &g, const Fields &F, const float *in, float *o1, float *o2, float *o3, cudaStream_t s) {
-    k_tti_dplus<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, in, o1, o2, o3);
-}
-
-void tti_dminus(const Grid &g, const Fields &F, const float *i1, const float *i2, const float *i3, float *o1,
-                float *o2, float *o3, cudaStream_t s) {
-    k_tti_dminus<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, i1, i2, i3, o1, o2, o3);
 }
 
 void born_iso(const Grid &g, int which, const Fields &F, const float *dv, const float *db, const float *dp,
@@ -569,23 +637,9 @@ void born_iso(const Grid &g, int which, const Fields &F, const float *dv, const 
     k_born_iso<<<blocks_for(g.n), kThreads, 0, s>>>(g, which, F, dv, db, dp, L);
 }
 
-void born_iso_scaleb(const Grid &g, const float *db, const float *const *t1, float *const *t2, cudaStream_t s) {
-    k_born_iso_scaleb<<<blocks_for(g.n), kThreads, 0, s>>>(g, db, p3(t1), m3(t2));
-}
-
 void born_aniso_v(const Grid &g, const Fields &F, const float *dv, const float *dp, const float *dm,
                   cudaStream_t s) {
     k_born_aniso_v<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dv, dp, dm);
-}
-
-void born_vea_sandwich(const Grid &g, const Fields &F, const float *de, const float *da, const float *const *tp1,
-                       const float *const *tm1, float *const *tp2, float *const *tm2, cudaStream_t s) {
-    k_born_vea_sandwich<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, de, da, p3(tp1), p3(tm1), m3(tp2), m3(tm2));
-}
-
-void born_vea_final(const Grid &g, const Fields &F, const float *dv, const float *dp, const float *dm,
-                    const float *const *lp, const float *const *lm, cudaStream_t s) {
-    k_born_vea_final<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dv, dp, dm, p3(lp), p3(lm));
 }
 
 void image_iso(const Grid &g, int which, const Fields &F, const float *dp, const float *const *t1,
@@ -599,10 +653,34 @@ void image_aniso_v(const Grid &g, const Fields &F, const float *dp, const float 
     k_image_aniso_v<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dp, dm, dv);
 }
 
-void image_vea(const Grid &g, const Fields &F, const float *dp, const float *dm, const float *const *tp1,
-               const float *const *tm1, const float *const *tp2, const float *const *tm2, float *dv, float *de,
-               float *da, cudaStream_t s) {
-    k_image_vea<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dp, dm, p3(tp1), p3(tm1), p3(tp2), p3(tm2), dv, de, da);
+void born_iso_fused(const Grid &g, int which, const Fields &F, const float *dv, const float *db, const float *P,
+                    const float *dp, float *const *t, cudaStream_t s) {
+    k_born_iso_b1<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, db, P, m3(t));
+    k_born_iso_b2<<<blocks_for(g.n), kThreads, 0, s>>>(g, which, F, dv, db, dp, p3(t));
+}
+
+void image_iso_fused(const Grid &g, int which, const Fields &F, const float *dp, const float *P, float *dv, float *db,
+                     cudaStream_t s) {
+    k_image_iso_b<<<blocks_for(g.n), kThreads, 0, s>>>(g, which, F, dp, P, dv, db);
+}
+
+void born_vea_fused(const Grid &g, bool rot, const Fields &F, const float *dv, const float *de, const float *da,
+                    const float *P, const float *M, const float *dp, const float *dm, float *const *t,
+                    cudaStream_t s) {
+    const unsigned nb = blocks_for(g.n);
+    if (rot) {
+        k_born_vea_1<true><<<nb, kThreads, 0, s>>>(g, F, de, da, P, M, m3(t), m3(t + 3));
+        k_born_vea_2<true><<<nb, kThreads, 0, s>>>(g, F, dv, dp, dm, p3(t), p3(t + 3));
+    } else {
+        k_born_vea_1<false><<<nb, kThreads, 0, s>>>(g, F, de, da, P, M, m3(t), m3(t + 3));
+        k_born_vea_2<false><<<nb, kThreads, 0, s>>>(g, F, dv, dp, dm, p3(t), p3(t + 3));
+    }
+}
+
+void image_vea_fused(const Grid &g, bool rot, const Fields &F, const float *dp, const float *dm, const float *P,
+                     const float *M, float *dv, float *de, float *da, cudaStream_t s) {
+    if (rot) k_image_vea_f<true><<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dp, dm, P, M, dv, de, da);
+    else k_image_vea_f<false><<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dp, dm, P, M, dv, de, da);
 }
 
 }  // namespace WFD_NS

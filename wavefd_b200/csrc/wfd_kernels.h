@@ -105,7 +105,6 @@ struct TileInfo {
        inside the step kernel */                                                                         \
     int fused_step(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s);      \
     void scale(const wfd::Grid &g, const wfd::Fields &F, bool two, cudaStream_t s);                      \
-    void dplus(const wfd::Grid &g, const float *in, float *ox, float *oy, float *oz, cudaStream_t s);    \
     void dplus3(const wfd::Grid &g, const float *inx, const float *iny, const float *inz, float *ox,     \
                 float *oy, float *oz, cudaStream_t s);                                                   \
     bool fused_iso3d(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                          \
@@ -139,30 +138,26 @@ struct TileInfo {
     void vti3d_set_pipeline_wait(unsigned long long ns);                                                 \
     void aniso3d_set_pipeline_wait(unsigned long long ns);                                               \
     void fused_set_pipeline_wait(unsigned long long ns);                                                 \
-    void dminus3(const wfd::Grid &g, const float *fx, const float *fy, const float *fz, float *ox,       \
-                 float *oy, float *oz, cudaStream_t s);                                                  \
-    void tti_dplus(const wfd::Grid &g, const wfd::Fields &F, const float *in, float *o1, float *o2,      \
-                   float *o3, cudaStream_t s);                                                           \
-    void tti_dminus(const wfd::Grid &g, const wfd::Fields &F, const float *i1, const float *i2,          \
-                    const float *i3, float *o1, float *o2, float *o3, cudaStream_t s);                   \
     void born_iso(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dv, const float *db, \
                   const float *dp, const float *const *lap, cudaStream_t s);                            \
-    void born_iso_scaleb(const wfd::Grid &g, const float *db, const float *const *t1, float *const *t2,  \
-                         cudaStream_t s);                                                                \
     void born_aniso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dv, const float *dp,        \
                       const float *dm, cudaStream_t s);                                                  \
-    void born_vea_sandwich(const wfd::Grid &g, const wfd::Fields &F, const float *de, const float *da,   \
-                           const float *const *tp1, const float *const *tm1, float *const *tp2,          \
-                           float *const *tm2, cudaStream_t s);                                           \
-    void born_vea_final(const wfd::Grid &g, const wfd::Fields &F, const float *dv, const float *dp,      \
-                        const float *dm, const float *const *lp, const float *const *lm, cudaStream_t s); \
     void image_iso(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dp,                 \
                    const float *const *t1, const float *const *t2, float *dv, float *db, cudaStream_t s); \
     void image_aniso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dp, const float *dm,       \
                        float *dv, cudaStream_t s);                                                       \
-    void image_vea(const wfd::Grid &g, const wfd::Fields &F, const float *dp, const float *dm,           \
-                   const float *const *tp1, const float *const *tm1, const float *const *tp2,            \
-                   const float *const *tm2, float *dv, float *de, float *da, cudaStream_t s);            \
+    /* the VB/B and VEA Born injections and imaging conditions with the gradient triples and their D-  \
+       formed per cell (t: 3 scratch arrays for born_iso_fused, 6 for born_vea_fused) */                 \
+    void born_iso_fused(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dv,            \
+                        const float *db, const float *P, const float *dp, float *const *t, cudaStream_t s); \
+    void image_iso_fused(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dp,          \
+                         const float *P, float *dv, float *db, cudaStream_t s);                          \
+    void born_vea_fused(const wfd::Grid &g, bool rot, const wfd::Fields &F, const float *dv,             \
+                        const float *de, const float *da, const float *P, const float *M, const float *dp, \
+                        const float *dm, float *const *t, cudaStream_t s);                              \
+    void image_vea_fused(const wfd::Grid &g, bool rot, const wfd::Fields &F, const float *dp,            \
+                         const float *dm, const float *P, const float *M, float *dv, float *de, float *da, \
+                         cudaStream_t s);                                                                \
     void image_wavefieldsep(const wfd::Grid &g, long isfwi, const wfd::Fields &F, const float *dp,       \
                             const float *dm, float *dv, float2 *work, long ncols_per_pass,               \
                             cudaStream_t s);                                                             \
