@@ -220,6 +220,68 @@ def test_imaging_strict_bitwise(lib, oracle, name, variant, fs):
 
 
 @pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("variant", ["VB", "B", "VEA"])
+def test_born_imaging_fast_close(lib, oracle, name, variant):
+    """The fast build (FMA contraction, approximate division) of the VB/B/VEA Born injections and
+    imaging conditions, whose gradient triples and D- are formed per cell: what each call adds to
+    pCur/mCur or to the images, against the checker's, relative L2 <= 1e-5."""
+    physics = PROPAGATORS[name][1]
+    if variant not in PROPAGATORS[name][3]:
+        pytest.skip("variant not defined for this physics")
+    tti = physics == "tti"
+    # Born injection
+    gpu, orc = _pair(lib, oracle, name, True, strict=False)
+    shp = orc.arr("V").shape
+    dv, db, de, da = _rand(shp, 51), _rand(shp, 52), _rand(shp, 53), _rand(shp, 54)
+    P, DP, M, DM = _rand(shp, 55), _rand(shp, 56), _rand(shp, 57), _rand(shp, 58)
+    keys = ["PCur"] if physics == "iso" else ["PCur", "MCur"]
+    before = {k: orc.arr(k).copy() for k in keys}
+    a = orc.a
+    fn = getattr(gpu.abi, "ForwardBornInjection_" + variant)
+    if physics == "iso":
+        args = {"VB": (dv, db, P, DP), "B": (db, P, DP)}[variant]
+        fn(gpu.p, *[fptr(x) for x in args])
+        oracle.born_iso(orc.g, {"VB": 1, "B": 2}[variant], a["V"], a["B"], dv, db, P, DP, a["PCur"])
+    else:
+        fn(gpu.p, *[fptr(x) for x in (dv, de, da, P, M, DP, DM)])
+        oracle.born_vea(orc.g, tti, a["V"], a["Eps"], a["Eta"], a["B"], a["F"], a["SinTheta"] if tti else None,
+                        a["CosTheta"] if tti else None, a["SinPhi"], a["CosPhi"], dv, de, da, P, M, DP, DM,
+                        a["PCur"], a["MCur"])
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(gpu.p)) == 0
+    for k in keys:
+        err = rel_l2(gpu.arr(k) - before[k], orc.arr(k) - before[k])
+        assert err <= 1e-5, f"{name} Born {variant} {k}: rel L2 of the increment {err:.2e}"
+    gpu.close()
+    # imaging condition
+    if variant not in PROPAGATORS[name][4]:
+        return
+    gpu, orc = _pair(lib, oracle, name, True, strict=False)
+    img = {k: _rand(shp, 60 + i) for i, k in enumerate(("v", "b", "e", "a"))}
+    start = {k: v.copy() for k, v in img.items()}
+    mine = {k: v.copy() for k, v in img.items()}
+    a = orc.a
+    fn = getattr(gpu.abi, "AdjointBornAccumulation_" + variant)
+    if physics == "iso":
+        if variant == "VB":
+            fn(gpu.p, fptr(img["v"]), fptr(img["b"]), fptr(P), fptr(DP))
+        else:
+            fn(gpu.p, fptr(img["b"]), fptr(P), fptr(DP))
+        oracle.image_iso(orc.g, {"VB": 1, "B": 2}[variant], a["V"], a["B"], P, DP, a["POld"], mine["v"], mine["b"])
+        ks = {"VB": ["v", "b"], "B": ["b"]}[variant]
+    else:
+        fn(gpu.p, *[fptr(x) for x in (img["v"], img["e"], img["a"], P, M, DP, DM)])
+        oracle.image_vea(orc.g, tti, a["V"], a["Eps"], a["Eta"], a["B"], a["F"], a["SinTheta"] if tti else None,
+                         a["CosTheta"] if tti else None, a["SinPhi"], a["CosPhi"], P, M, DP, DM, a["POld"],
+                         a["MOld"], mine["v"], mine["e"], mine["a"])
+        ks = ["v", "e", "a"]
+    assert lib.WFD_Prop_Status(ctypes.c_void_p(gpu.p)) == 0
+    for k in ks:
+        err = rel_l2(img[k] - start[k], mine[k] - start[k])
+        assert err <= 1e-5, f"{name} imaging {variant} {k}: rel L2 of the increment {err:.2e}"
+    gpu.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("isfwi", [0, 1])
 @pytest.mark.parametrize("nz", [26, 32])  # Bluestein length and power-of-two length
 def test_wavefieldsep_close(lib, oracle, name, isfwi, nz):
