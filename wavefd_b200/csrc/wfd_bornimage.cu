@@ -84,9 +84,9 @@ struct K {
         if (strict) wfd_strict::fn(a...);                                     \
         else wfd_fast::fn(a...);                                              \
     }
-    WFD_DISPATCH(born_iso)
+    WFD_DISPATCH(born_iso_v)
     WFD_DISPATCH(born_aniso_v)
-    WFD_DISPATCH(image_iso)
+    WFD_DISPATCH(image_iso_v)
     WFD_DISPATCH(image_aniso_v)
     WFD_DISPATCH(image_wavefieldsep)
     WFD_DISPATCH(born_iso_fused)
@@ -116,7 +116,7 @@ int prop_born(Prop *p, const char *variant, float *const *args, int nargs) {
     float **t = p->tmp;
     if (p->phys == ISO) {
         if (!strcmp(variant, "V")) {
-            k.born_iso(g, 0, F, a[0], (const float *)nullptr, a[1], (const float *const *)nullptr, p->stream);
+            k.born_iso_v(g, F, a[0], a[1], p->stream);
         } else {
             const bool vb = !strcmp(variant, "VB");
             float *dv = vb ? a[0] : nullptr, *db = vb ? a[1] : a[0], *P = vb ? a[2] : a[1], *DP = vb ? a[3] : a[2];
@@ -156,8 +156,7 @@ int prop_image(Prop *p, const char *variant, float *const *args, int nargs, long
         outs.push_back(a[0]);
     } else if (p->phys == ISO) {
         if (!strcmp(variant, "V")) {
-            k.image_iso(g, 0, F, a[1], (const float *const *)nullptr, (const float *const *)nullptr, a[0],
-                        (float *)nullptr, p->stream);
+            k.image_iso_v(g, F, a[1], a[0], p->stream);
             outs.push_back(a[0]);
         } else {
             const bool vb = !strcmp(variant, "VB");

@@ -283,54 +283,27 @@ __global__ void __launch_bounds__(kThreads) k_dplus(Grid g, const float *__restr
 }
 
 // ---------------------------------------------------------------------------------------------
-// Born injection. Iso V: 3D .h:305-334, 2D .h:253-280 (a different expression);
-// Iso VB/B final loops: 3D .h:389-416 / .h:471-497 and the 2D forms.
+// Born injection V, Iso: 3D .h:305-334, 2D .h:253-280 (a different expression)
 struct Ptr3 {
     const float *p[3];
 };
 struct MPtr3 {
     float *p[3];
 };
-__global__ void __launch_bounds__(kThreads) k_born_iso(Grid g, int which, Fields F, const float *__restrict__ dv,
-                                                       const float *__restrict__ db, const float *__restrict__ dp,
-                                                       Ptr3 L) {
+__global__ void __launch_bounds__(kThreads) k_born_iso_v(Grid g, Fields F, const float *__restrict__ dv,
+                                                         const float *__restrict__ dp) {
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= g.n) return;
     const float V = F.v[k], B = F.b[k];
     const float dt = g.dt;
-    if (which == 0) {
-        const float dV = dv[k];
-        if (g.ndim == 3) {
-            const float dt2v2OverB = dt * dt * V * V / B;
-            const float factorV = 2 * B * dV / (V * V * V);
-            F.pcur[k] += dt2v2OverB * dp[k] * factorV;
-        } else {
-            const float factor = 2 * dt * dt * dV / V;
-            F.pcur[k] += factor * dp[k];
-        }
-        return;
-    }
-    const float dB = db[k];
+    const float dV = dv[k];
     if (g.ndim == 3) {
         const float dt2v2OverB = dt * dt * V * V / B;
-        const float factorB = -dB / (V * V);
-        if (which == 1) {
-            const float dV = dv[k];
-            const float factorV = 2 * B * dV / (V * V * V);
-            F.pcur[k] += dt2v2OverB * (dp[k] * (factorV + factorB) + L.p[0][k] + L.p[1][k] + L.p[2][k]);
-        } else {
-            F.pcur[k] += dt2v2OverB * (dp[k] * factorB + L.p[0][k] + L.p[1][k] + L.p[2][k]);
-        }
+        const float factorV = 2 * B * dV / (V * V * V);
+        F.pcur[k] += dt2v2OverB * dp[k] * factorV;
     } else {
-        const float V2 = V * V;
-        const float dt2v2OverB = dt * dt * V2 / B;
-        if (which == 1) {
-            const float dV = dv[k];
-            F.pcur[k] += dt2v2OverB * (dp[k] / V2 * (2 * B * dV / V - dB) + L.p[0][k] + L.p[2][k]);
-        } else {
-            const float factorB = -dB / V2;
-            F.pcur[k] += dt2v2OverB * (dp[k] * factorB + L.p[0][k] + L.p[2][k]);
-        }
+        const float factor = 2 * dt * dt * dV / V;
+        F.pcur[k] += factor * dp[k];
     }
 }
 
@@ -347,24 +320,13 @@ __global__ void __launch_bounds__(kThreads) k_born_aniso_v(Grid g, Fields F, con
 }
 
 // ---------------------------------------------------------------------------------------------
-// Imaging conditions. Iso V/VB/B: 3D .h:518-656 and the 2D forms.
-__global__ void __launch_bounds__(kThreads) k_image_iso(Grid g, int which, Fields F, const float *__restrict__ dp,
-                                                        Ptr3 t1, Ptr3 t2, float *dv, float *db) {
+// Imaging conditions. Iso V: 3D .h:518-546 and the 2D form.
+__global__ void __launch_bounds__(kThreads) k_image_iso_v(Grid g, Fields F, const float *__restrict__ dp, float *dv) {
     const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= g.n) return;
     const float V = F.v[k], B = F.b[k];
-    const float po = F.pold[k];
-    if (which == 0 || which == 1) {
-        const float factorV = +2 * B / (V * V * V);
-        dv[k] += factorV * dp[k] * po;
-    }
-    if (which != 0) {
-        const float factorB = -1 / (V * V);
-        if (g.ndim == 3)
-            db[k] += factorB * dp[k] * po - t1.p[0][k] * t2.p[0][k] - t1.p[1][k] * t2.p[1][k] - t1.p[2][k] * t2.p[2][k];
-        else
-            db[k] += factorB * dp[k] * po - t1.p[0][k] * t2.p[0][k] - t1.p[2][k] * t2.p[2][k];
-    }
+    const float factorV = +2 * B / (V * V * V);
+    dv[k] += factorV * dp[k] * F.pold[k];
 }
 
 // VTI/TTI V (3D VTI .h:564-589; 3D TTI .h:567-592; 2D alike)
@@ -631,10 +593,8 @@ void dplus3(const Grid &g, const float *inx, const float *iny, const float *inz,
     k_dplus<<<blocks_for(g.n), kThreads, 0, s>>>(g, inx, iny, inz, ox, oy, oz);
 }
 
-void born_iso(const Grid &g, int which, const Fields &F, const float *dv, const float *db, const float *dp,
-              const float *const *lap, cudaStream_t s) {
-    Ptr3 L = lap ? p3(lap) : Ptr3{{nullptr, nullptr, nullptr}};
-    k_born_iso<<<blocks_for(g.n), kThreads, 0, s>>>(g, which, F, dv, db, dp, L);
+void born_iso_v(const Grid &g, const Fields &F, const float *dv, const float *dp, cudaStream_t s) {
+    k_born_iso_v<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dv, dp);
 }
 
 void born_aniso_v(const Grid &g, const Fields &F, const float *dv, const float *dp, const float *dm,
@@ -642,11 +602,8 @@ void born_aniso_v(const Grid &g, const Fields &F, const float *dv, const float *
     k_born_aniso_v<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dv, dp, dm);
 }
 
-void image_iso(const Grid &g, int which, const Fields &F, const float *dp, const float *const *t1,
-               const float *const *t2, float *dv, float *db, cudaStream_t s) {
-    Ptr3 a = t1 ? p3(t1) : Ptr3{{nullptr, nullptr, nullptr}};
-    Ptr3 b = t2 ? p3(t2) : Ptr3{{nullptr, nullptr, nullptr}};
-    k_image_iso<<<blocks_for(g.n), kThreads, 0, s>>>(g, which, F, dp, a, b, dv, db);
+void image_iso_v(const Grid &g, const Fields &F, const float *dp, float *dv, cudaStream_t s) {
+    k_image_iso_v<<<blocks_for(g.n), kThreads, 0, s>>>(g, F, dp, dv);
 }
 
 void image_aniso_v(const Grid &g, const Fields &F, const float *dp, const float *dm, float *dv, cudaStream_t s) {

@@ -138,12 +138,12 @@ struct TileInfo {
     void vti3d_set_pipeline_wait(unsigned long long ns);                                                 \
     void aniso3d_set_pipeline_wait(unsigned long long ns);                                               \
     void fused_set_pipeline_wait(unsigned long long ns);                                                 \
-    void born_iso(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dv, const float *db, \
-                  const float *dp, const float *const *lap, cudaStream_t s);                            \
+    void born_iso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dv, const float *dp,          \
+                    cudaStream_t s);                                                                     \
     void born_aniso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dv, const float *dp,        \
                       const float *dm, cudaStream_t s);                                                  \
-    void image_iso(const wfd::Grid &g, int which, const wfd::Fields &F, const float *dp,                 \
-                   const float *const *t1, const float *const *t2, float *dv, float *db, cudaStream_t s); \
+    void image_iso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dp, float *dv,              \
+                     cudaStream_t s);                                                                    \
     void image_aniso_v(const wfd::Grid &g, const wfd::Fields &F, const float *dp, const float *dm,       \
                        float *dv, cudaStream_t s);                                                       \
     /* the VB/B and VEA Born injections and imaging conditions with the gradient triples and their D-  \

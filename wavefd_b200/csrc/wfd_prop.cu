@@ -365,9 +365,8 @@ int prop_step(Prop *p, bool linear, bool sync) {
         }
         if (e.born_dv) {
             if (iso) {
-                const float *lap[3] = {nullptr, nullptr, nullptr};
-                if (p->strict) wfd_strict::born_iso(g, 0, Fs, e.born_dv, nullptr, e.born_dp, lap, p->stream);
-                else wfd_fast::born_iso(g, 0, Fs, e.born_dv, nullptr, e.born_dp, lap, p->stream);
+                if (p->strict) wfd_strict::born_iso_v(g, Fs, e.born_dv, e.born_dp, p->stream);
+                else wfd_fast::born_iso_v(g, Fs, e.born_dv, e.born_dp, p->stream);
             } else if (p->strict) {
                 wfd_strict::born_aniso_v(g, Fs, e.born_dv, e.born_dp, e.born_dm, p->stream);
             } else {
@@ -377,9 +376,8 @@ int prop_step(Prop *p, bool linear, bool sync) {
         }
         if (e.img) {
             if (iso) {
-                const float *t[3] = {nullptr, nullptr, nullptr};
-                if (p->strict) wfd_strict::image_iso(g, 0, Fs, e.img_dp, t, t, e.img, nullptr, p->stream);
-                else wfd_fast::image_iso(g, 0, Fs, e.img_dp, t, t, e.img, nullptr, p->stream);
+                if (p->strict) wfd_strict::image_iso_v(g, Fs, e.img_dp, e.img, p->stream);
+                else wfd_fast::image_iso_v(g, Fs, e.img_dp, e.img, p->stream);
             } else if (p->strict) {
                 wfd_strict::image_aniso_v(g, Fs, e.img_dp, e.img_dm, e.img, p->stream);
             } else {
