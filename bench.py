@@ -48,6 +48,15 @@ WORKLOADS = {
                   label="2D AcoIsoDenQ forward, 501 x 501, 10 m, dt 1 ms, nt 2000, 60-cell sponge, constant Q "
                         "100, 15 Hz Ricker at the centre of the top row, receivers on every surface cell"),
     # profiling-size case of the same kernel (fields still larger than L2: 67 MB each)
+    # the fused 2D VTI and TTI steps on the same grid (the time loop as a CUDA graph of two steps)
+    "vti2d": dict(physics="vti", name="Prop2DAcoVTIDenQ_DEO2_FDTD", shape=(501, 1, 501), d=10.0, dt=0.0005,
+                  nt=2000, nsponge=60, fpeak=15.0, nrec=(501, 1), bytes_per_cell=56, ndim=2,
+                  label="2D AcoVTIDenQ forward, 501 x 501, 10 m, dt 0.5 ms, nt 2000, 60-cell sponge, "
+                        "receivers on every surface cell"),
+    "tti2d": dict(physics="tti", name="Prop2DAcoTTIDenQ_DEO2_FDTD", shape=(501, 1, 501), d=10.0, dt=0.0005,
+                  nt=2000, nsponge=60, fpeak=15.0, nrec=(501, 1), bytes_per_cell=64, ndim=2,
+                  label="2D AcoTTIDenQ forward, 501 x 501, 10 m, dt 0.5 ms, nt 2000, 60-cell sponge, "
+                        "receivers on every surface cell"),
     "iso256": dict(physics="iso", name="Prop3DAcoIsoDenQ_DEO2_FDTD", shape=(256, 256, 256), d=10.0, dt=0.0005,
                    nt=1000, nsponge=40, fpeak=12.0, nrec=(128, 128), bytes_per_cell=28,
                    label="3D AcoIsoDenQ forward, 256^3 (16.8M cells), profiling size"),
@@ -199,6 +208,8 @@ def run_ours(args, W):
                                   nsponge=W["nsponge"], device="cuda")
     # write the model into the object's managed arrays on the device (no host round trip)
     for k, t in model.items():
+        if W.get("ndim", 3) == 2 and k in ("SinPhi", "CosPhi"):
+            continue  # (2D TTI has no azimuth)
         dst = _managed_tensor(prop, k, (nx, ny, nz))
         dst.copy_(t)
     del model
@@ -969,7 +980,9 @@ def _ref_object(W, lib_name, fl, th, shape, nby, nbx):
         arr("Eta")[...] = 0.05
         arr("F")[...] = 0.85
     if W["physics"] == "tti":
-        for g, v in (("SinTheta", 0.3), ("CosTheta", 0.954), ("SinPhi", 0.5), ("CosPhi", 0.866)):
+        angles = (("SinTheta", 0.3), ("CosTheta", 0.954)) + (() if W.get("ndim", 3) == 2 else
+                                                               (("SinPhi", 0.5), ("CosPhi", 0.866)))
+        for g, v in angles:
             arr(g)[...] = v
     rng = np.random.default_rng(0)
     arr("PCur")[:, :, :64] = rng.standard_normal((nx, ny, min(64, nz))).astype(np.float32)[:, :, :64] * 1e-3
