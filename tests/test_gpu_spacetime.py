@@ -225,6 +225,8 @@ def test_illumination_bitwise(lib, oracle):
 
 
 @pytest.mark.parametrize("name,shape", [("Prop2DAcoIsoDenQ_DEO2_FDTD", (44, 1, 38)),
+                                        ("Prop2DAcoVTIDenQ_DEO2_FDTD", (44, 1, 38)),
+                                        ("Prop2DAcoTTIDenQ_DEO2_FDTD", (44, 1, 38)),
                                         ("Prop3DAcoTTIDenQ_DEO2_FDTD", (28, 22, 24))])
 @pytest.mark.parametrize("use_graph", [1, 0])
 def test_prop_run_matches_stepping(lib, name, shape, use_graph):
@@ -357,16 +359,20 @@ def test_illumination_fused_into_step(lib, name, shape):
 
 @pytest.mark.parametrize("spread", ["local", "far"])
 @pytest.mark.parametrize("shape", [(200, 1, 90), (1000, 1, 400)])
-def test_prop_run_2d_tiles(lib, spread, shape):
-    """The 2D Iso whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each),
+@pytest.mark.parametrize("name", ["Prop2DAcoIsoDenQ_DEO2_FDTD", "Prop2DAcoVTIDenQ_DEO2_FDTD",
+                                  "Prop2DAcoTTIDenQ_DEO2_FDTD"])
+def test_prop_run_2d_tiles(lib, spread, shape, name):
+    """The 2D whole-loop launch on a grid of many tiles in both directions (16 x 64 cells each),
     receiver groups of two points one row apart or 40 rows apart (more than two tiles), sources in one
     tile, on a tile corner, on the free-surface rows and outside the interior (cells the step does
     not write), against TimeStep + WFD_Inject + WFD_Extract per step, bitwise (strict build). At
     200 x 90 (24 tiles) every tile stays in one CTA for the whole loop; at 1000 x 400 (400 tiles,
-    more than the CTAs that fit at once) the CTAs take turns over the tiles."""
+    more than the CTAs that fit at once) the CTAs take turns over the tiles (2D Iso; the 2D VTI and TTI
+    loop always shares the tiles out over the CTAs)."""
     import torch
     from tests.harness import ABIRunner, make_model
-    name = "Prop2DAcoIsoDenQ_DEO2_FDTD"
+    from wavefd_b200.abi import PROPAGATORS
+    physics = PROPAGATORS[name][1]
     nz, ny, nx = shape
     nt, nsteps = 40, 17
     gap = nz * (1 if spread == "local" else 40)  # the second point of a group: 1 or 40 rows further in x
@@ -379,7 +385,7 @@ def test_prop_run_2d_tiles(lib, spread, shape):
     for mode in ("run", "steps"):
         g = ABIRunner(lib, name, shape, fs=True)
         lib.WFD_Prop_SetStrict(ctypes.c_void_p(g.p), 1)
-        g.load(make_model(2, "iso", shape, seed=8))
+        g.load(make_model(2, physics, shape, seed=8))
         h = nx // 2
         spts = [SourcePoint32(h * nz + 3, 1, 1.0),             # free-surface row kz 2
                 SourcePoint32(h * nz + 6, 2, 0.5),             # the same tile
@@ -407,7 +413,8 @@ def test_prop_run_2d_tiles(lib, spread, shape):
                 assert lib.WFD_Extract(tr, ctypes.c_void_p(trc.data_ptr()), pc, it, nt, stream) == 0
         assert lib.WFD_Prop_Synchronize(ctypes.c_void_p(g.p)) == 0
         assert lib.WFD_Prop_Status(ctypes.c_void_p(g.p)) == 0
-        runs.append(({k: g.arr(k).copy() for k in ("PCur", "POld", "PSpace")}, trc.cpu().numpy()))
+        keys = ("PCur", "POld", "PSpace") + (() if physics == "iso" else ("MCur", "MOld", "MSpace"))
+        runs.append(({k: g.arr(k).copy() for k in keys}, trc.cpu().numpy()))
         lib.WFD_Points_Free(ts)
         lib.WFD_Points_Free(tr)
         g.close()

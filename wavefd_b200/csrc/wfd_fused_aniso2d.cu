@@ -12,6 +12,7 @@
 // the symmetric image above the free surface by reflecting the column index (t[-j] = t[j-1], the
 // weights of the TTI back-rotation with it). Cell arithmetic is the expression trees of the
 // two-pass kernels (wfd_generic.cu), so the strict build gives their bits.
+#include "wfd_gridbar.cuh"
 #include "wfd_kernels.h"
 
 namespace WFD_NS {
@@ -48,15 +49,24 @@ __device__ __forceinline__ float stm(const Grid &g, const W &w) {
     return g.c1 * (-w(-1) + w(0)) + g.c2 * (-w(-2) + w(1)) + g.c3 * (-w(-3) + w(2)) + g.c4 * (-w(-4) + w(3));
 }
 
-template <int PHYS, bool LINEAR>
-__global__ void __launch_bounds__(NT) k_aniso2d_fused(Grid g, Fields F) {
-    extern __shared__ __align__(16) float sm[];
+// loads of the fields a step writes: past L1 in the whole-loop launch (other CTAs rewrite them
+// between steps)
+template <bool RUN>
+__device__ __forceinline__ float ldf(const float *p) {
+    return RUN ? __ldcg(p) : *p;
+}
+
+// One step of the tile at (x0, z0) (shared memory sm of SMEM_BYTES); in the whole-loop launch
+// (RUN) also the step's source injection at time index it into the tile's cells of the new pCur,
+// each group's contributions in order, separate IEEE multiply and add, as the injection kernel does.
+template <int PHYS, bool LINEAR, bool RUN>
+__device__ __forceinline__ void aniso_tile_step(const Grid &g, const Fields &F, const long x0, const long z0,
+                                                float *sm, const long it) {
     float(*P)[PZW] = reinterpret_cast<float(*)[PZW]>(sm + O_PM);
     float(*Mf)[PZW] = reinterpret_cast<float(*)[PZW]>(sm + O_PM + PXH * PZW);
     auto mat = [&](int m) { return reinterpret_cast<float(*)[MZW]>(sm + O_MAT + m * MXH * MZW); };
     auto out = [&](int o) { return reinterpret_cast<float(*)[OZW]>(sm + O_OUT + o * OXH * OZW); };
     const int tz = threadIdx.x % WZ, tx = threadIdx.x / WZ;
-    const long z0 = (long)blockIdx.x * TZ, x0 = (long)blockIdx.y * TX;
     const long nx = g.nx, nz = g.nz;
     constexpr int nmat = PHYS == TTI ? 6 : 4;
 
@@ -69,11 +79,11 @@ __global__ void __launch_bounds__(NT) k_aniso2d_fused(Grid g, Fields F) {
             float vp = 0.0f, vm = 0.0f;
             if (xin) {
                 if (z >= 0 && z < nz) {
-                    vp = F.pcur[x * nz + z];
-                    vm = F.mcur[x * nz + z];
+                    vp = ldf<RUN>(F.pcur + x * nz + z);
+                    vm = ldf<RUN>(F.mcur + x * nz + z);
                 } else if (z < 0 && -z < nz) {
-                    vp = -F.pcur[x * nz - z];
-                    vm = -F.mcur[x * nz - z];
+                    vp = -ldf<RUN>(F.pcur + x * nz - z);
+                    vm = -ldf<RUN>(F.mcur + x * nz - z);
                 }
             }
             P[r][c] = vp;
@@ -216,10 +226,64 @@ __global__ void __launch_bounds__(NT) k_aniso2d_fused(Grid g, Fields F) {
             const float V = F.v[k];
             const float dt2V2_B = g.dt2 * V * V / F.b[k];
             const float Q = F.q[k];
-            const float pc = F.pcur[k], po = F.pold[k];
-            const float mc = F.mcur[k], mo = F.mold[k];
+            const float pc = ldf<RUN>(F.pcur + k), po = ldf<RUN>(F.pold + k);
+            const float mc = ldf<RUN>(F.mcur + k), mo = ldf<RUN>(F.mold + k);
             F.pold[k] = dt2V2_B * LP - Q * (pc - po) - po + 2 * pc;
             F.mold[k] = dt2V2_B * LM - Q * (mc - mo) - mo + 2 * mc;
+        }
+    }
+    if (RUN && F.inj.ngroups && it >= 1 && it <= F.inj.nt) {
+        __syncthreads();
+        for (long gi = threadIdx.x; gi < F.inj.ngroups; gi += NT) {
+            const long key = F.inj.key[gi];
+            const long x = key / nz, z = key - x * nz;
+            if (x < x0 || x >= x0 + TX || z < z0 || z >= z0 + TZ) continue;
+            float acc = __ldcg(F.pold + key);
+            for (long j = F.inj.start[gi]; j < F.inj.start[gi + 1]; j++)
+                acc = __fadd_rn(acc, __fmul_rn(F.inj.c[j], F.inj.wav[F.inj.other[j] * F.inj.nt + (it - 1)]));
+            F.pold[key] = acc;
+        }
+    }
+}
+
+template <int PHYS, bool LINEAR>
+__global__ void __launch_bounds__(NT) k_aniso2d_fused(Grid g, Fields F) {
+    extern __shared__ __align__(16) float sm[];
+    aniso_tile_step<PHYS, LINEAR, false>(g, F, (long)blockIdx.y * TX, (long)blockIdx.x * TZ, sm, 0);
+}
+
+// A whole 2D VTI or TTI time loop in one cooperative launch, as k_iso2d_run for 2D Iso: per step
+// every tile's step with its source injection (CTAs take turns over the tiles), a grid-wide barrier,
+// then the receiver extraction from the new pCur; the pointer swaps of every step are the
+// alternation of the two arrays of each field.
+template <int PHYS>
+__global__ void __launch_bounds__(NT) k_aniso2d_run(Grid g, Fields F, long nsteps, long it0, RunExtract ex,
+                                                    unsigned *sync_words) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ int ok_flag;
+    const long ntz = (g.nz + TZ - 1) / TZ, ntx = (g.nx + TX - 1) / TX, ntiles = ntz * ntx;
+    unsigned gen = 0;
+    for (long st = 0; st < nsteps; st++) {
+        Fields Fs = F;
+        Fs.pcur = (st & 1) ? F.pold : F.pcur;
+        Fs.pold = (st & 1) ? F.pcur : F.pold;
+        Fs.mcur = (st & 1) ? F.mold : F.mcur;
+        Fs.mold = (st & 1) ? F.mcur : F.mold;
+        const long it = it0 + st;
+        for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            aniso_tile_step<PHYS, false, true>(g, Fs, (t / ntz) * TX, (t % ntz) * TZ, sm, it);
+            __syncthreads();  // the tile's shared memory is reused by the next tile
+        }
+        if (!grid_barrier(sync_words, gen, &ok_flag)) return;
+        if (ex.ngroups && it >= 1 && it <= ex.nt) {
+            // data[key*nt + it-1] += sum c * new pCur[other], each group in order, IEEE multiply and add
+            for (long gi = (long)blockIdx.x * NT + threadIdx.x; gi < ex.ngroups; gi += (long)gridDim.x * NT) {
+                float *dst = ex.data + ex.key[gi] * ex.nt + (it - 1);
+                float acc = *dst;
+                for (long j = ex.start[gi]; j < ex.start[gi + 1]; j++)
+                    acc = __fadd_rn(acc, __fmul_rn(ex.c[j], __ldcg(Fs.pold + ex.other[j])));
+                *dst = acc;
+            }
         }
     }
 }
@@ -240,6 +304,35 @@ bool launch2(const Grid &g, const Fields &F, cudaStream_t s) {
 }
 
 }  // namespace
+
+int aniso2d_run(const Grid &g, int phys, const Fields &F, long nsteps, long it0, const RunExtract &ex,
+                unsigned *sync_words, cudaStream_t s) {
+    if (g.ndim != 2 || (phys != VTI && phys != TTI)) return -1;
+    // co-resident CTAs (0: no cooperative launch, or the shared memory cannot be granted)
+    static int cap[2] = {-1, -1};
+    const int which = phys == TTI ? 1 : 0;
+    const void *fn = which ? (const void *)k_aniso2d_run<TTI> : (const void *)k_aniso2d_run<VTI>;
+    if (cap[which] < 0) {
+        int dev = 0, sms = 0, per = 0, coop = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) == cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, NT, SMEM_BYTES);
+        cudaGetLastError();
+        cap[which] = coop ? sms * per : 0;
+    }
+    if (cap[which] <= 0) return -1;
+    const long ntiles = ((g.nz + TZ - 1) / TZ) * ((g.nx + TX - 1) / TX);
+    const int grid = (int)(ntiles < cap[which] ? ntiles : cap[which]);
+    Grid gg = g;
+    Fields FF = F;
+    long ns = nsteps, i0 = it0;
+    RunExtract ee = ex;
+    unsigned *sw = sync_words;
+    void *args[] = {&gg, &FF, &ns, &i0, &ee, &sw};
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), args, SMEM_BYTES, s) == cudaSuccess ? 0 : 1;
+}
 
 bool fused_aniso2d(const Grid &g, int phys, int linear, const Fields &F, cudaStream_t s) {
     if (g.ndim != 2) return false;

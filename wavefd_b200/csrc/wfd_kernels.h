@@ -113,6 +113,9 @@ struct TileInfo {
     /* whole 2D Iso time loop in one cooperative launch: 0 launched, -1 not available, 1 launch error */ \
     int iso2d_run(const wfd::Grid &g, const wfd::Fields &F, long nsteps, long it0, const wfd::RunExtract &ex, \
                   unsigned *sync_words, cudaStream_t s);                                                 \
+    /* the same for 2D VTI and TTI (phys), the tiles shared out over the co-resident CTAs */           \
+    int aniso2d_run(const wfd::Grid &g, int phys, const wfd::Fields &F, long nsteps, long it0,          \
+                    const wfd::RunExtract &ex, unsigned *sync_words, cudaStream_t s);                    \
     bool fused_iso3d_tma(const wfd::Grid &g, const wfd::Fields &F, cudaStream_t s);                      \
     bool fused_aniso3d_tma(const wfd::Grid &g, int phys, int linear, const wfd::Fields &F, cudaStream_t s); \
     bool fused_vti3d_tma(const wfd::Grid &g, int linear, const wfd::Fields &F, cudaStream_t s);         \

@@ -437,8 +437,7 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     // scratch of the unfused passes must exist before a capture (no allocation inside a graph)
     if (!p->fused || p->ndim == 2 || p->nz % 4 != 0)
         if (!wfd::ensure_scratch(p, p->phys == wfd::ISO ? 3 : 6)) return p->status;
-    const bool run2d = p->ndim == 2 && p->phys == wfd::ISO && p->fused && !p->illum && nsteps > 0 &&
-                       (!src || src->t.ngroups <= 1024);
+    const bool run2d = p->ndim == 2 && p->fused && !p->illum && nsteps > 0 && (!src || src->t.ngroups <= 1024);
     long *d_it = nullptr;
     // d_it[0]: the time index; d_it[1]: the finished-block count of the extraction launch;
     // d_it[2..3]: the barrier words of the persistent 2D loop (count, generation, status)
@@ -447,7 +446,7 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
     const long init[4] = {it0, 0, 0, 0};
     cudaMemcpyAsync(d_it, init, sizeof init, cudaMemcpyHostToDevice, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, "time index upload");
-    // 2D Iso: the whole loop in one cooperative launch (grid-wide barrier between steps)
+    // 2D: the whole loop in one cooperative launch (grid-wide barrier between steps)
     if (run2d) {
         wfd::Fields F = p->fields();
         F.inj = wfd::StepInject{};
@@ -459,8 +458,13 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
             ex = wfd::RunExtract{rec->t.ngroups, rec->t.d_key, rec->t.d_start, rec->t.d_other, rec->t.d_c, traces, nt};
         unsigned *words = reinterpret_cast<unsigned *>(d_it + 2);
         const wfd::Grid g = p->grid();
-        const int r = p->strict ? wfd_strict::iso2d_run(g, F, nsteps, it0, ex, words, s)
-                                : wfd_fast::iso2d_run(g, F, nsteps, it0, ex, words, s);
+        int r;
+        if (p->phys == wfd::ISO)
+            r = p->strict ? wfd_strict::iso2d_run(g, F, nsteps, it0, ex, words, s)
+                          : wfd_fast::iso2d_run(g, F, nsteps, it0, ex, words, s);
+        else
+            r = p->strict ? wfd_strict::aniso2d_run(g, p->phys, F, nsteps, it0, ex, words, s)
+                          : wfd_fast::aniso2d_run(g, p->phys, F, nsteps, it0, ex, words, s);
         if (r == 0) {
             unsigned status = 0;
             cudaMemcpyAsync(&status, words + 2, sizeof status, cudaMemcpyDeviceToHost, s);
@@ -468,7 +472,10 @@ extern "C" int WFD_Prop_Run(void *prop, long nsteps, long it0, void *src_table, 
             cudaFreeAsync(d_it, s);
             if (e != cudaSuccess) return wfd::prop_fail(p, WFD_ERR_CUDA, std::string("time loop: ") + cudaGetErrorString(e));
             if (status) return wfd::prop_fail(p, WFD_ERR_TIMEOUT, "time loop: a grid-wide barrier timed out");
-            if (nsteps & 1) std::swap(p->field[wfd::F_PCUR], p->field[wfd::F_POLD]);
+            if (nsteps & 1) {
+                std::swap(p->field[wfd::F_PCUR], p->field[wfd::F_POLD]);
+                if (p->phys != wfd::ISO) std::swap(p->field[wfd::F_MCUR], p->field[wfd::F_MOLD]);
+            }
             p->steps += nsteps;
             p->step_kernels = 1;
             p->run_launches = 1;
