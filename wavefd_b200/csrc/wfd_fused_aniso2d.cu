@@ -59,9 +59,10 @@ __device__ __forceinline__ float ldf(const float *p) {
 // One step of the tile at (x0, z0) (shared memory sm of SMEM_BYTES); in the whole-loop launch
 // (RUN) also the step's source injection at time index it into the tile's cells of the new pCur,
 // each group's contributions in order, separate IEEE multiply and add, as the injection kernel does.
+// load_mat false: the material boxes are those of this tile from the step before.
 template <int PHYS, bool LINEAR, bool RUN>
 __device__ __forceinline__ void aniso_tile_step(const Grid &g, const Fields &F, const long x0, const long z0,
-                                                float *sm, const long it) {
+                                                float *sm, const long it, const bool load_mat = true) {
     float(*P)[PZW] = reinterpret_cast<float(*)[PZW]>(sm + O_PM);
     float(*Mf)[PZW] = reinterpret_cast<float(*)[PZW]>(sm + O_PM + PXH * PZW);
     auto mat = [&](int m) { return reinterpret_cast<float(*)[MZW]>(sm + O_MAT + m * MXH * MZW); };
@@ -91,7 +92,7 @@ __device__ __forceinline__ void aniso_tile_step(const Grid &g, const Fields &F, 
         }
     }
     const float *msrc[NMAT_MAX] = {F.b, F.eps, F.eta, F.f, F.st, F.ct};
-    for (int m = 0; m < nmat; m++) {
+    for (int m = 0; m < nmat && load_mat; m++) {  // (already in shared memory when the tile stays)
         float(*Ms)[MZW] = mat(m);
         for (int r = tx; r < MXH; r += WX) {
             const long x = x0 - 4 + r;
@@ -253,9 +254,10 @@ __global__ void __launch_bounds__(NT) k_aniso2d_fused(Grid g, Fields F) {
 }
 
 // A whole 2D VTI or TTI time loop in one cooperative launch, as k_iso2d_run for 2D Iso: per step
-// every tile's step with its source injection (CTAs take turns over the tiles), a grid-wide barrier,
-// then the receiver extraction from the new pCur; the pointer swaps of every step are the
-// alternation of the two arrays of each field.
+// every tile's step with its source injection (CTAs take turns over the tiles; with as many CTAs as
+// tiles each keeps its tile and its material boxes), a grid-wide barrier, then the receiver
+// extraction from the new pCur; the pointer swaps of every step are the alternation of the two
+// arrays of each field.
 template <int PHYS>
 __global__ void __launch_bounds__(NT) k_aniso2d_run(Grid g, Fields F, long nsteps, long it0, RunExtract ex,
                                                     unsigned *sync_words) {
@@ -271,7 +273,9 @@ __global__ void __launch_bounds__(NT) k_aniso2d_run(Grid g, Fields F, long nstep
         Fs.mold = (st & 1) ? F.mcur : F.mold;
         const long it = it0 + st;
         for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            aniso_tile_step<PHYS, false, true>(g, Fs, (t / ntz) * TX, (t % ntz) * TZ, sm, it);
+            // a CTA with one tile for the whole loop keeps the tile's material boxes
+            aniso_tile_step<PHYS, false, true>(g, Fs, (t / ntz) * TX, (t % ntz) * TZ, sm, it,
+                                               st == 0 || gridDim.x != ntiles);
             __syncthreads();  // the tile's shared memory is reused by the next tile
         }
         if (!grid_barrier(sync_words, gen, &ok_flag)) return;
